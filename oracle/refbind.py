@@ -1,0 +1,158 @@
+"""ctypes binding of the compiled reference (oracle/_ref/libspmref.so).
+
+TEST INFRASTRUCTURE ONLY: the reference's own src/*.cpp built unchanged against
+the shims in oracle/shim (see oracle/Makefile and oracle/ref_harness.cpp).
+Tests, __graft_entry__.smoke() and bench.py's CPU baseline / reference arm use
+it as the checker or the timed CPU reference; the product never loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libspmref.so")
+REFDIR_DEFAULT = "/root/reference"
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+
+def build(refdir: str = REFDIR_DEFAULT, quiet: bool = True) -> bool:
+    """Compile the oracle with its Makefile when the reference tree is present."""
+    if not os.path.isdir(os.path.join(refdir, "src")):
+        return os.path.exists(LIB)
+    out = subprocess.run(["make", "-C", HERE, f"REFDIR={refdir}"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    return True
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(LIB)
+        L = ctypes.CDLL(LIB)
+        L.ref_setup.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_get_Ene.restype = ctypes.c_double
+        L.ref_inpfp.restype = ctypes.c_double
+        L.ref_rayleighq.restype = ctypes.c_double
+        L.ref_get_GK.restype = ctypes.c_double
+        L.ref_get_GK.argtypes = [ctypes.c_double]
+        L.ref_lobpcg_init.argtypes = [ctypes.c_int, ctypes.c_uint64, _dp]
+        L.ref_lobpcg_inip.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_spring_pairing.argtypes = [_dp, _dp, ctypes.c_double, ctypes.c_double]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+class Ref:
+    """One configured reference instance (the reference keeps its state in globals)."""
+
+    def __init__(self, N, L=26.0, Tau=-0.0061, Gamma=0.30, dt=0.3, threads=1):
+        self.N, self.n3 = N, N ** 3
+        self.L = lib()
+        self.L.ref_set_threads(int(threads))
+        if self.L.ref_setup(N, L, Tau, Gamma, dt) != 0:
+            raise ValueError("ref_setup failed")
+
+    def _z(self, k=1):
+        return np.zeros((k, self.N, self.N, self.N)) if k > 1 else np.zeros((self.N,) * 3)
+
+    def tables(self):
+        G, ik = self._z(), self._z()
+        self.L.ref_get_tables(_p(G), _p(ik))
+        return G, ik
+
+    def set_state(self, phi, uF=None):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        if uF is None:
+            self.L.ref_set_state(_p(phi))
+        else:
+            uFi = np.ascontiguousarray(np.stack([uF.real, uF.imag], axis=-1))
+            self.L.ref_set_state2(_p(phi), _p(uFi))
+
+    def get_state(self):
+        phi = self._z()
+        uFi = np.zeros((self.N, self.N, self.N, 2))
+        self.L.ref_get_state(_p(phi), _p(uFi))
+        return phi, uFi[..., 0] + 1j * uFi[..., 1]
+
+    def energy(self):
+        return self.L.ref_get_Ene()
+
+    def grad_steps(self, n):
+        E, res, g = np.zeros(n), np.zeros(n), np.zeros(n)
+        self.L.ref_grad_steps(n, _p(E), _p(res), _p(g))
+        return E, res, g
+
+    def get_min_u_F(self, maxit):
+        self.L.ref_get_min_u_F(int(maxit))
+
+    def ngrad(self, phi):
+        out = self._z()
+        self.L.ref_ngrad(_p(np.ascontiguousarray(phi)), _p(out))
+        return out
+
+    def hv(self, phi, v):
+        out = self._z()
+        self.L.ref_hv(_p(np.ascontiguousarray(phi)), _p(np.ascontiguousarray(v)), _p(out))
+        return out
+
+    def precond(self, w):
+        w = np.array(w, dtype=np.float64, order="C")
+        self.L.ref_precond(_p(w))
+        return w
+
+    def inpfp(self, p, q):
+        return self.L.ref_inpfp(_p(np.ascontiguousarray(p)), _p(np.ascontiguousarray(q)))
+
+    def rayleigh(self, phi, v):
+        return self.L.ref_rayleighq(_p(np.ascontiguousarray(phi)), _p(np.ascontiguousarray(v)))
+
+    def lobpcg_init(self, k, seed):
+        V = self._z(k) if k > 1 else np.zeros((1, self.N, self.N, self.N))
+        self.L.ref_lobpcg_init(k, seed, _p(V))
+        return V
+
+    def lobpcg_inip(self, phi, V, maxiter=21):
+        V = np.array(V, dtype=np.float64, order="C")
+        self.L.ref_lobpcg_inip(_p(np.ascontiguousarray(phi)), V.shape[0], int(maxiter), _p(V))
+        return V
+
+    def tangent(self, phi0, phi1):
+        out = self._z()
+        self.L.ref_get_Tv(_p(np.ascontiguousarray(phi0)), _p(np.ascontiguousarray(phi1)), _p(out))
+        return out
+
+    def natural_forces(self, x, v):
+        x = np.array(x, dtype=np.float64, order="C")
+        self.L.ref_natural_forces(_p(x), _p(np.ascontiguousarray(v)))
+        return x
+
+    def minmax_forces(self, x, v):
+        x = np.array(x, dtype=np.float64, order="C")
+        self.L.ref_minmax_forces(_p(x), _p(np.ascontiguousarray(v)))
+        return x
+
+    def spring_pairing(self, phi0, phi1, maxiter, tol):
+        a = np.array(phi0, dtype=np.float64, order="C")
+        b = np.array(phi1, dtype=np.float64, order="C")
+        self.L.ref_spring_pairing(_p(a), _p(b), float(maxiter), float(tol))
+        return a, b
+
+    def close(self):
+        self.L.ref_teardown()
