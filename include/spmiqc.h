@@ -1,0 +1,130 @@
+/* spmiqc.h -- C ABI of the B200 (sm_100a) implementation of SPM-IQC's
+ * pseudo-spectral hot path (libspmiqc_cuda.so).
+ *
+ * The reference (JKGroupCUDA/SPM-IQC) has no plugin API: its hot path is a set
+ * of free C++ functions over process globals. Each entry point below names the
+ * reference routine it replaces (file:line within the SPM-IQC project). The
+ * C++ signatures themselves are kept by the link-time compat layer declared in
+ * spmiqc_compat.h.
+ *
+ * Conventions
+ *  - Every function returns an int status (SPM_OK = 0, else SPM_ERR_*); the
+ *    reference returns void and aborts on MPI errors. spm_last_error() gives
+ *    a message for the calling thread.
+ *  - A context owns one grid size N, the model parameters and its scratch; it
+ *    is bound to one CUDA device and one stream and is not re-entrant (one
+ *    context per thread), like the reference's globals.
+ *  - "Field" arguments are device pointers to real arrays of N^3 values of the
+ *    context's precision (double for SPM_FP64, float for SPM_FP32), row-major
+ *    i*N*N + j*N + k, the reference's index order (Initialization.cpp:109-120).
+ *    Batched entry points take nb fields stored back to back.
+ *  - "Spectrum" arguments are device pointers to the packed half spectrum:
+ *    N*N*(N/2) complex values (re, im interleaved), spec[(kx*N + ky)*(N/2) + c]
+ *    = X(kx, ky, c) for c >= 1 and X(kx, ky, 0) + i X(kx, ky, N/2) for c = 0,
+ *    where X is the reference's spectrum, normalised by 1/N^3
+ *    (My_FFT.cpp:4-13). spm_spectrum_to_full / _from_full convert to and from
+ *    the reference's full N^3 complex layout.
+ *  - Norms and inner products follow inpfp/nrmp: <p,q> = (1/N^3) sum p q
+ *    (BasicOperators.cpp:132-172); ||grad F|| = nrmp(ngrad_cam(phi)).
+ *  - Functions run asynchronously on the context's stream unless they return a
+ *    host scalar, in which case they synchronise the stream.
+ */
+#ifndef SPMIQC_H
+#define SPMIQC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spm_ctx spm_ctx;
+
+enum spm_status {
+  SPM_OK = 0,
+  SPM_ERR_ARG = 1,          /* bad argument (size, null pointer, batch) */
+  SPM_ERR_CUDA = 2,         /* a CUDA runtime error */
+  SPM_ERR_NOMEM = 3,        /* device allocation refused */
+  SPM_ERR_NONFINITE = 4,    /* a reduction returned NaN/Inf */
+  SPM_ERR_UNSUPPORTED = 5,  /* grid size or precision not built */
+  SPM_ERR_STATE = 6         /* call order (e.g. LOBPCG block not initialised) */
+};
+
+enum spm_precision { SPM_FP64 = 0, SPM_FP32 = 1 };
+
+/* Per-step record of a gradient-flow run (LPsrc.cpp:52-110). */
+typedef struct spm_step_stats {
+  double energy;    /* get_Ene() of the state entering the step (LPsrc.cpp:54) */
+  double res;       /* max_k |Re(u'_k - u_k)| (LPsrc.cpp:77-84) */
+  double grad_norm; /* nrmp(ngrad_cam(phi)) of the state entering the step */
+  double e1;        /* the pair-interaction part 1/2 sum G |u|^2 */
+} spm_step_stats;
+
+/* ---------------------------------------------------------------- context */
+
+/* Creates a context for an N^3 grid. Replaces the set-up of main_SPM.cpp:29-60
+ * (LPsystParameter, get_kindex_all, My_mpi_fft_set_up, get_ksquare_local,
+ * get_epmckt2_local, get_ikt2_local): k^2, G(k) and the preconditioner symbol
+ * are evaluated inside the kernels, so no tables are built. stream may be NULL
+ * (the legacy default stream). N must satisfy spm_supported_size(N). */
+int spm_ctx_create(int N, double L, double Tau, double Gamma, double dt, int precision,
+                   void *stream, spm_ctx **out);
+int spm_ctx_destroy(spm_ctx *ctx);
+int spm_set_stream(spm_ctx *ctx, void *stream);
+int spm_sync(spm_ctx *ctx);
+int spm_supported_size(int N);
+size_t spm_field_bytes(const spm_ctx *ctx);
+size_t spm_spectrum_bytes(const spm_ctx *ctx);
+const char *spm_status_str(int status);
+const char *spm_last_error(void);
+/* Number of transform-kernel launches issued by this context so far. */
+uint64_t spm_launch_count(const spm_ctx *ctx);
+
+/* ------------------------------------------------------------- transforms */
+
+/* my_fft (My_FFT.cpp:4-13): xhat = FFT(x) / N^3, packed. */
+int spm_fft(spm_ctx *ctx, const void *x, void *xhat);
+/* my_ifft (My_FFT.cpp:15-21): x = unnormalised inverse of xhat. */
+int spm_ifft(spm_ctx *ctx, const void *xhat, void *x);
+/* Packed spectrum <-> the reference's full N^3 complex spectrum
+ * (fftw_complex, interleaved, always double). */
+int spm_spectrum_to_full(spm_ctx *ctx, const void *xhat, double *full);
+int spm_spectrum_from_full(spm_ctx *ctx, const double *full, void *xhat);
+
+/* ------------------------------------------------------ energy / gradient */
+
+/* get_Ene (LPsrc.cpp:8-38) on the state (phi, uhat) as given. */
+int spm_energy(spm_ctx *ctx, const void *phi, const void *uhat, double *energy);
+
+/* get_min_u_F (LPsrc.cpp:40-117): up to max_steps semi-implicit steps on
+ * (phi, uhat) in place. The loop stops after the step whose res <= 1e-16 (the
+ * reference's criterion) or, when tol_grad > 0, after the first step whose
+ * incoming state has ||grad F|| <= tol_grad. stats (host, may be NULL) receives
+ * one record per executed step; *steps_done the number of steps executed.
+ * Steps are enqueued ahead in chunks and stop on the device, so no host round
+ * trip happens per step. */
+int spm_grad_flow(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol_grad,
+                  spm_step_stats *stats, int *steps_done);
+
+/* ngrad_cam (LPsrc.cpp:119-173): grad = -grad F(phi). If norm is non-NULL it
+ * receives nrmp(grad) (synchronises). */
+int spm_ngrad(spm_ctx *ctx, const void *phi, void *grad, double *norm);
+
+/* ---------------------------------------------------- Hessian / precond */
+
+/* hv_cam (LOBPCG.cpp:113-166) for nb vectors: hv[b] = H(phi) v[b]. */
+int spm_hv(spm_ctx *ctx, const void *phi, const void *v, void *hv, int nb);
+/* precond_camnew (LOBPCG.cpp:168-199), in place on nb vectors. */
+int spm_precond(spm_ctx *ctx, void *w, int nb);
+
+/* ------------------------------------------------------------ BLAS-1 */
+
+/* inpfp (BasicOperators.cpp:132-143): <p, q> = (1/N^3) sum p q. */
+int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPMIQC_H */

@@ -1,0 +1,310 @@
+// Building blocks of the sm_100a pseudo-spectral kernels: complex helpers,
+// in-register mixed-radix DFTs (radix 2, 3, 4, 5 and their products up to 16),
+// deterministic block / grid reductions, and the shared parameter block.
+//
+// The 3D transform replaces FFTW's C2C (src/My_FFT.cpp:4-21 of SPM-IQC) with a
+// real-to-complex transform in "packed" layout: for a real N^3 field the
+// spectrum is stored as N x N x (N/2) complex values, spec[kx][ky][c]:
+//   c >= 1 : X(kx, ky, kz = c)                        (the half spectrum)
+//   c == 0 : X(kx, ky, 0) + i * X(kx, ky, N/2)        (both planes Hermitian)
+// so a spectrum takes exactly as many bytes as the real field. The forward
+// transform is unnormalised here; ops apply the reference's 1/N^3.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace cg = cooperative_groups;
+
+namespace spm {
+
+#include "tw240.inc"
+
+constexpr int kThreads = 256;   // threads per CTA in every transform kernel
+constexpr int kRows = 32;       // z-lines (rows of an x-plane) per CTA, plane kernels
+constexpr int kCols = 16;       // y-lines (spectral columns) per CTA, plane kernels
+constexpr int kMaxBatch = 16;   // fields per launch
+constexpr int kScal = 16;       // scalars per field in the scalar block
+constexpr int kRedMax = 8;      // reduction slots per field and CTA
+constexpr int kPartStride = 2048;  // CTAs per field reserved in the partials buffer
+
+// Scalar-block slots (per field): results of reductions, inputs of later kernels.
+enum Slot {
+  SC_E2 = 0,    // mean of the local free-energy density (LPsrc.cpp:19-24)
+  SC_E1 = 1,    // 1/2 sum_k G |u_k|^2 (LPsrc.cpp:27-35)
+  SC_RES = 2,   // max |Re(u'_k - u_k)| (LPsrc.cpp:77-84)
+  SC_GN2 = 3,   // ||grad F||^2
+  SC_MU = 4,    // mean removed by an epilogue (the P0 projector)
+  SC_S = 5,     // <f, v> projection coefficient of the SPM force steps
+  SC_NRM2 = 6,  // squared norm (tangent)
+  SC_SUM0 = 8,  // raw sums for host-side use
+  SC_SUM1 = 9,
+  SC_SUM2 = 10,
+  SC_SUM3 = 11,
+};
+
+template <class T> struct V2;
+template <> struct V2<double> { using type = double2; };
+template <> struct V2<float> { using type = float2; };
+template <class T> using c2 = typename V2<T>::type;
+
+template <class T2> using base_t = decltype(T2::x);
+
+template <class T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return {a.x + b.x, a.y + b.y}; }
+template <class T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) { return {a.x - b.x, a.y - b.y}; }
+template <class T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <class T2> __device__ __forceinline__ T2 cmulc(T2 a, T2 b) {  // a * conj(b)
+  return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <class T2> __device__ __forceinline__ T2 cconj(T2 a) { return {a.x, -a.y}; }
+template <class T2, class S> __device__ __forceinline__ T2 cscale(T2 a, S s) {
+  return {a.x * s, a.y * s};
+}
+// a * (D * i), D = +-1
+template <int D, class T2> __device__ __forceinline__ T2 mul_di(T2 a) {
+  if constexpr (D > 0) return {-a.y, a.x};
+  else return {a.y, -a.x};
+}
+
+// compile-time loop: f(std::integral_constant<int, I>) for I in [B, E)
+template <int B, int E, class F> __device__ __forceinline__ void sfor(F &&f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    sfor<B + 1, E>(f);
+  }
+}
+#define SPM_CI(x) decltype(x)::value
+
+// v * exp(DIR * 2 pi i * E / P) with E, P compile-time; exact for multiples of pi/2.
+template <int DIR, int P, int E, class T2> __device__ __forceinline__ T2 twc(T2 v) {
+  constexpr int e = ((E % P) + P) % P;
+  if constexpr (e == 0) {
+    return v;
+  } else if constexpr (4 * e == P) {
+    return mul_di<DIR>(v);
+  } else if constexpr (2 * e == P) {
+    return {-v.x, -v.y};
+  } else if constexpr (4 * e == 3 * P) {
+    return mul_di<-DIR>(v);
+  } else {
+    static_assert(240 % P == 0, "radix must divide 240");
+    using T = base_t<T2>;
+    constexpr T c = (T)kTw240[e * (240 / P)][0];
+    constexpr T s = (T)(DIR * kTw240[e * (240 / P)][1]);
+    return {v.x * c - v.y * s, v.x * s + v.y * c};
+  }
+}
+
+// In-place DFT of P register values, natural order in and out:
+//   X[k] = sum_j v[j] exp(DIR * 2 pi i j k / P).
+template <int DIR, int P, class T2> struct Dft;
+
+template <int DIR, class T2> struct Dft<DIR, 1, T2> {
+  static __device__ __forceinline__ void run(T2 (&)[1]) {}
+};
+template <int DIR, class T2> struct Dft<DIR, 2, T2> {
+  static __device__ __forceinline__ void run(T2 (&v)[2]) {
+    T2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <int DIR, class T2> struct Dft<DIR, 3, T2> {
+  static __device__ __forceinline__ void run(T2 (&v)[3]) {
+    using T = base_t<T2>;
+    constexpr T h = (T)0.8660254037844386467637232;  // sqrt(3)/2
+    T2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    T2 x0 = cadd(v[0], t1);
+    T2 m = {v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
+    T2 n = mul_di<DIR>(cscale(t2, h));
+    v[0] = x0;
+    v[1] = cadd(m, n);
+    v[2] = csub(m, n);
+  }
+};
+template <int DIR, class T2> struct Dft<DIR, 4, T2> {
+  static __device__ __forceinline__ void run(T2 (&v)[4]) {
+    T2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    T2 t2 = cadd(v[1], v[3]), t3 = mul_di<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[2] = csub(t0, t2);
+    v[3] = csub(t1, t3);
+  }
+};
+template <int DIR, class T2> struct Dft<DIR, 5, T2> {
+  static __device__ __forceinline__ void run(T2 (&v)[5]) {
+    using T = base_t<T2>;
+    constexpr T c1 = (T)kTw240[48][0], c2 = (T)kTw240[96][0];
+    constexpr T s1 = (T)kTw240[48][1], s2 = (T)kTw240[96][1];
+    T2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    T2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    T2 x0 = cadd(v[0], cadd(t1, t2));
+    T2 b1 = {v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y};
+    T2 b2 = {v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y};
+    T2 d1 = mul_di<DIR>(T2{s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y});
+    T2 d2 = mul_di<DIR>(T2{s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y});
+    v[0] = x0;
+    v[1] = cadd(b1, d1);
+    v[4] = csub(b1, d1);
+    v[2] = cadd(b2, d2);
+    v[3] = csub(b2, d2);
+  }
+};
+// Composite P = A * B (Cooley-Tukey): j = j1*B + j2, k = k1 + A*k2.
+template <int DIR, int P, class T2> struct Dft {
+  static constexpr int A = (P % 4 == 0 && P > 4) ? 4 : (P % 2 == 0 ? 2 : (P % 3 == 0 ? 3 : 5));
+  static constexpr int B = P / A;
+  static_assert(A * B == P && B > 1, "unsupported radix");
+  static __device__ __forceinline__ void run(T2 (&v)[P]) {
+    T2 u[A][B];
+    sfor<0, B>([&](auto J2) {
+      constexpr int j2 = SPM_CI(J2);
+      T2 t[A];
+      sfor<0, A>([&](auto J1) { t[SPM_CI(J1)] = v[SPM_CI(J1) * B + j2]; });
+      Dft<DIR, A, T2>::run(t);
+      sfor<0, A>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        u[k1][j2] = twc<DIR, P, k1 * j2>(t[k1]);
+      });
+    });
+    sfor<0, A>([&](auto K1) {
+      constexpr int k1 = SPM_CI(K1);
+      T2 t[B];
+      sfor<0, B>([&](auto J2) { t[SPM_CI(J2)] = u[k1][SPM_CI(J2)]; });
+      Dft<DIR, B, T2>::run(t);
+      sfor<0, B>([&](auto K2) { v[k1 + A * SPM_CI(K2)] = t[SPM_CI(K2)]; });
+    });
+  }
+};
+
+// ------------------------------------------------------------------ reductions
+// Slot r of a reduction is a max when bit r of MAXM is set, otherwise a sum.
+template <int NR, unsigned MAXM>
+__device__ __forceinline__ void combine(double (&a)[NR], const double (&b)[NR]) {
+#pragma unroll
+  for (int r = 0; r < NR; r++) a[r] = ((MAXM >> r) & 1u) ? fmax(a[r], b[r]) : a[r] + b[r];
+}
+
+// Deterministic block reduction (fixed butterfly + fixed warp order).
+// The result is valid in thread 0. scratch: 32 * NR doubles of shared memory.
+template <int NR, unsigned MAXM>
+__device__ __forceinline__ void block_reduce(double (&a)[NR], double *scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    double b[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) b[r] = __shfl_xor_sync(0xffffffffu, a[r], off);
+    combine<NR, MAXM>(a, b);
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int r = 0; r < NR; r++) scratch[warp * NR + r] = a[r];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int w = 1; w < nw; w++) {
+      double b[NR];
+#pragma unroll
+      for (int r = 0; r < NR; r++) b[r] = scratch[w * NR + r];
+      combine<NR, MAXM>(a, b);
+    }
+  }
+}
+
+// Grid reduction: every CTA writes its block total to partials[bidx]; the CTA
+// that finishes last sums all partials in fixed index order (so the result does
+// not depend on scheduling) and returns true in its thread 0 with tot filled.
+template <int NR, unsigned MAXM>
+__device__ __forceinline__ bool grid_reduce(double (&acc)[NR], double *scratch, double *partials,
+                                            unsigned *ticket, int nblk, int bidx, double (&tot)[NR]) {
+  __shared__ int s_last;
+  block_reduce<NR, MAXM>(acc, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) partials[(size_t)bidx * kRedMax + r] = acc[r];
+    __threadfence();
+    unsigned prev = atomicAdd(ticket, 1u);
+    s_last = (prev == (unsigned)nblk - 1u);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double a[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) a[r] = ((MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    double b[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) b[r] = __ldcg(&partials[(size_t)i * kRedMax + r]);
+    combine<NR, MAXM>(a, b);
+  }
+  block_reduce<NR, MAXM>(a, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) tot[r] = a[r];
+    *ticket = 0u;
+    return true;
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------ parameters
+struct ModelC {
+  double Tau, Gamma, dt;
+  double invL;     // 1/L, the reference's projection entry (Initialization.cpp:35-38)
+  double inv_n3;   // 1/N^3
+  double n3;
+  double G0;       // G(k = 0)
+  double ikt0;     // 1/(G0 + |Tau| + 0.02)
+  double tol_grad; // grad-flow stop threshold on ||grad F|| (<= 0: off)
+  double factor;   // SPM projection factor: 1 natural force, 2 min-max
+};
+
+// Grad-flow control words in device memory.
+enum FlowWord { FW_GO = 0, FW_PENDING = 1, FW_ITER = 2 };
+
+struct KParams {
+  ModelC m;
+  const void *in[kMaxBatch];
+  void *out[kMaxBatch];
+  const void *aux0[kMaxBatch];
+  const void *aux1[kMaxBatch];
+  const void *st[kMaxBatch];
+  void *sto[kMaxBatch];
+  const void *tw;       // T2[N]: exp(-2 pi i j / N)
+  double *partials;     // [nb][blocks per field][kRedMax]
+  unsigned *tickets;    // [nb]
+  double *scal;         // [nb][kScal]
+  int *flow;            // grad-flow control words (or null)
+  double *stats;        // grad-flow per-step records (or null)
+  int nb;
+};
+
+// Signed wave number of index i on an N grid (Initialization.cpp:97-107).
+__device__ __forceinline__ int wave(int i, int N) { return i < N / 2 ? i : i - N; }
+
+// Pair kernel G at integer wave vector (Kx, Ky, Kz): k^2 = ((px^2 + py^2) + pz^2),
+// p = K / L as the reference builds it (Initialization.cpp:132-148), then
+// get_GK (Initialization.cpp:150-166). Rounded multiplies/adds keep the k^2
+// arithmetic identical to the reference's; exp is CUDA's.
+__device__ __forceinline__ double gk_of(int Kx, int Ky, int Kz, double invL) {
+  double px = __dmul_rn(invL, (double)Kx), py = __dmul_rn(invL, (double)Ky),
+         pz = __dmul_rn(invL, (double)Kz);
+  double k2 = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
+  const double ph = 0.568809;
+  const double s2 = ph * ph;
+  double k4 = k2 * k2, k6 = k4 * k2, k8 = k6 * k2;
+  double poly = 1.969182919080340 + -14.949858723012090 * k2 + 37.445683882581790 * k4 +
+                -38.839451762550148 * k6 + 13.999261011773505 * k8;
+  return exp(-0.5 * k2 / s2) * poly + 0.08;
+}
+
+}  // namespace spm

@@ -1,0 +1,361 @@
+// Pointwise policies that specialise the three transform passes into the
+// reference's hot-path routines. Each policy cites the SPM-IQC code it follows.
+#pragma once
+
+#include "fft_kernels.cuh"
+
+namespace spm {
+
+template <class T> __device__ __forceinline__ const T *fld(const void *p) { return reinterpret_cast<const T *>(p); }
+__device__ __forceinline__ double *scal_of(const KParams &p, int b) { return p.scal + (size_t)b * kScal; }
+
+// ===================================================================== prologues
+// Transform the field as it is; no reduction.
+template <class T> struct ProIdent {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &, int, size_t, c2<T> x, double (&)[1]) { return x; }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Gradient step (LPsrc.cpp:44-75): transform f = Tau u + Gamma u^2 - u^3 and sum
+// the local energy density -Tau/2 u^2 - Gamma/3 u^3 + u^4/4 (LPsrc.cpp:10-24).
+template <class T> struct ProGrad {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, double (&acc)[1]) {
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    c2<T> f;
+    {
+      const T u = x.x, u2 = u * u, u3 = u2 * u, u4 = u3 * u;
+      acc[0] += (double)(-(T)0.5 * tau * u2 - gam * u3 / (T)3 + (T)0.25 * u4);
+      f.x = tau * u + gam * u2 - u3;
+    }
+    {
+      const T u = x.y, u2 = u * u, u3 = u2 * u, u4 = u3 * u;
+      acc[0] += (double)(-(T)0.5 * tau * u2 - gam * u3 / (T)3 + (T)0.25 * u4);
+      f.y = tau * u + gam * u2 - u3;
+    }
+    return f;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_E2] = tot[0] * p.m.inv_n3;
+  }
+};
+
+// Hessian-vector product (LOBPCG.cpp:113-166): transform v; accumulate sum(v)
+// and sum((-Tau - 2 Gamma phi + 3 phi^2) v) so the epilogue can remove the mean
+// mu = G(0) mean(v) + mean(c(phi) v) without a second pass (aux0 = phi).
+template <class T> struct ProHv {
+  static constexpr int NR = 2;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[2]) {
+    const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    acc[0] += (double)x.x + (double)x.y;
+    acc[1] += (double)((-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * x.x);
+    acc[1] += (double)((-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * x.y);
+    return x;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[2]) {
+    scal_of(p, b)[SC_MU] = p.m.G0 * (tot[0] * p.m.inv_n3) + tot[1] * p.m.inv_n3;
+  }
+};
+
+// Negative gradient (LPsrc.cpp:119-173): transform phi; accumulate sum(f),
+// f = Tau phi + Gamma phi^2 - phi^3, whose mean is the mean the reference
+// subtracts (the G-term has zero mean because its k = 0 mode is removed).
+template <class T> struct ProNgrad {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, double (&acc)[1]) {
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    acc[0] += (double)(tau * x.x + gam * x.x * x.x - x.x * x.x * x.x);
+    acc[0] += (double)(tau * x.y + gam * x.y * x.y - x.y * x.y * x.y);
+    return x;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_MU] = tot[0] * p.m.inv_n3;
+  }
+};
+
+// Preconditioner (LOBPCG.cpp:168-199): transform w; the epilogue removes the
+// mean ikt2(0) * mean(w).
+template <class T> struct ProPrecond {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &, int, size_t, c2<T> x, double (&acc)[1]) {
+    acc[0] += (double)x.x + (double)x.y;
+    return x;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_MU] = p.m.ikt0 * (tot[0] * p.m.inv_n3);
+  }
+};
+
+// SPM force step (SPM.cpp:34-99, 103-168) with beta = 1. Transforms
+// T = x + N(x), N = Tau x + Gamma x^2 - x^3 (its mean only touches the k = 0
+// mode, which the step zeroes), and accumulates the projection
+//   <f, v> = -<x, Gv> + <N, v> - mean(N) mean(v),  f = ngrad(x),
+// where Gv = IFFT(G FFT(v), k = 0 removed) is prepared once per tangent.
+// aux0 = v, aux1 = Gv.
+template <class T> struct ProForce {
+  static constexpr int NR = 4;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[4]) {
+    const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const c2<T> gv = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    const T n0 = tau * x.x + gam * x.x * x.x - x.x * x.x * x.x;
+    const T n1 = tau * x.y + gam * x.y * x.y - x.y * x.y * x.y;
+    acc[0] += (double)x.x * (double)gv.x + (double)x.y * (double)gv.y;
+    acc[1] += (double)n0 * (double)v.x + (double)n1 * (double)v.y;
+    acc[2] += (double)n0 + (double)n1;
+    acc[3] += (double)v.x + (double)v.y;
+    return c2<T>{x.x + n0, x.y + n1};
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[4]) {
+    const double s = -tot[0] * p.m.inv_n3 + tot[1] * p.m.inv_n3 -
+                     (tot[2] * p.m.inv_n3) * (tot[3] * p.m.inv_n3);
+    scal_of(p, b)[SC_S] = p.m.factor * s;
+  }
+};
+
+// SPM tangent (SPM.cpp:15-32): transform d = Phi1 - Phi0 (in = Phi1, aux0 =
+// Phi0) and accumulate |d|^2; the pencil scales by 1/||d||.
+template <class T> struct ProTangent {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[1]) {
+    const c2<T> a = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const c2<T> d = {x.x - a.x, x.y - a.y};
+    acc[0] += (double)d.x * (double)d.x + (double)d.y * (double)d.y;
+    return d;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_NRM2] = tot[0] * p.m.inv_n3;
+  }
+};
+
+// ===================================================================== pencil ops
+// Forward transform with the reference's 1/N^3 (My_FFT.cpp:9-13): store only.
+template <class T> struct OpFwd {
+  static constexpr bool FI = true, SI = false, SO = true, INV = false, LIN = true;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int, int, int, int, c2<T> f, c2<T>, c2<T> &so, c2<T> &,
+                               double (&)[1], double) {
+    so = cscale(f, (T)p.m.inv_n3);
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Backward transform of a stored spectrum (My_FFT.cpp:15-21): inverse only.
+template <class T> struct OpInv {
+  static constexpr bool FI = false, SI = true, SO = false, INV = true, LIN = true;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &, int, int, int, int, c2<T>, c2<T> s, c2<T> &, c2<T> &inv,
+                               double (&)[1], double) {
+    inv = s;
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// One semi-implicit gradient step (LPsrc.cpp:64-84) with the energy and
+// ||grad F|| of the incoming state:
+//   u' = (dt f^ + u) / (1 + dt G), u'_0 = 0,  res = max |Re(u' - u)|,
+//   E1 = 1/2 sum G |u|^2,  ||grad F||^2 = sum_{k != 0} |G u - f^|^2.
+template <class T> struct OpGrad {
+  static constexpr bool FI = true, SI = true, SO = true, INV = true, LIN = false;
+  static constexpr int NR = 3;
+  static constexpr unsigned MAXM = 0x2;
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &so,
+                               c2<T> &inv, double (&acc)[3], double w) {
+    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    const T Gt = (T)G;
+    const T dt = (T)p.m.dt;
+    const c2<T> fh = cscale(f, (T)p.m.inv_n3);
+    const T den = (T)1 + dt * Gt;
+    c2<T> u1 = {(dt * fh.x + s.x) / den, (dt * fh.y + s.y) / den};
+    const bool k0 = (Kx == 0 && Ky == 0 && Kz == 0);
+    if (k0) u1 = c2<T>{0, 0};
+    acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
+    acc[1] = fmax(acc[1], fabs((double)u1.x - (double)s.x));
+    if (!k0) {
+      const double gx = G * (double)s.x - (double)fh.x, gy = G * (double)s.y - (double)fh.y;
+      acc[2] += w * (gx * gx + gy * gy);
+    }
+    so = u1;
+    inv = u1;
+  }
+  // Record (E, res, ||grad F||) of this step; arm the stop when the reference's
+  // criterion res <= 1e-16 (LPsrc.cpp:52) or ||grad F|| <= tol_grad holds.
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[3]) {
+    double *sc = scal_of(p, b);
+    const double E = tot[0] + sc[SC_E2];
+    const double gn = sqrt(tot[2]);
+    sc[SC_E1] = tot[0];
+    sc[SC_RES] = tot[1];
+    sc[SC_GN2] = tot[2];
+    if (p.flow) {
+      const int it = p.flow[FW_ITER];
+      if (p.stats) {
+        p.stats[4 * it + 0] = E;
+        p.stats[4 * it + 1] = tot[1];
+        p.stats[4 * it + 2] = gn;
+        p.stats[4 * it + 3] = tot[0];
+      }
+      p.flow[FW_ITER] = it + 1;
+      if (!(tot[1] > 1e-16) || (p.m.tol_grad > 0 && gn <= p.m.tol_grad)) p.flow[FW_PENDING] = 1;
+    }
+  }
+};
+
+// G multiply for the Hessian-vector product (LOBPCG.cpp:126-134; the k = 0
+// mode is kept) or, with ZERO_DC, for ngrad_cam (LPsrc.cpp:133-142).
+template <class T, bool ZERO_DC> struct OpGmul {
+  static constexpr bool FI = true, SI = false, SO = false, INV = true, LIN = false;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
+                               c2<T> &inv, double (&)[1], double) {
+    const T g = (T)gk_of(Kx, Ky, Kz, p.m.invL);
+    inv = cscale(cscale(f, (T)p.m.inv_n3), g);
+    if (ZERO_DC && Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Preconditioner symbol 1/(G + |Tau| + 0.02) (Initialization.cpp:123-129, LOBPCG.cpp:175-179).
+template <class T> struct OpPrecond {
+  static constexpr bool FI = true, SI = false, SO = false, INV = true, LIN = false;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
+                               c2<T> &inv, double (&)[1], double) {
+    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    const T ik = (T)(1.0 / (G + fabs(p.m.Tau) + 0.02));
+    inv = cscale(cscale(f, (T)p.m.inv_n3), ik);
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// SPM force update (SPM.cpp:82-91): x'^ = (x^ + N^ - s v^) / (1 + G), x'^_0 = 0,
+// with s = factor * <ngrad(x), v> from the prologue and v^ (st) the stored
+// spectrum of the tangent.
+template <class T> struct OpForce {
+  static constexpr bool FI = true, SI = true, SO = false, INV = true, LIN = false;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &,
+                               c2<T> &inv, double (&)[1], double) {
+    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    const T sc = (T)scal_of(p, b)[SC_S];
+    const T den = (T)1 + (T)G;
+    const c2<T> fh = cscale(f, (T)p.m.inv_n3);
+    inv = c2<T>{(fh.x - sc * s.x) / den, (fh.y - sc * s.y) / den};
+    if (Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Tangent spectrum v^ = FFT(d) / (N^3 ||d||) (stored) and the G-weighted
+// field Gv = IFFT(G v^, k = 0 removed) (inverse output).
+template <class T> struct OpTangent {
+  static constexpr bool FI = true, SI = false, SO = true, INV = true, LIN = false;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &so,
+                               c2<T> &inv, double (&)[1], double) {
+    const T inrm = (T)(1.0 / sqrt(scal_of(p, b)[SC_NRM2]));
+    const c2<T> v = cscale(cscale(f, (T)p.m.inv_n3), inrm);
+    so = v;
+    const T g = (T)gk_of(Kx, Ky, Kz, p.m.invL);
+    inv = (Kx == 0 && Ky == 0 && Kz == 0) ? c2<T>{0, 0} : cscale(v, g);
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// E1 = 1/2 sum_k G |u_k|^2 of a stored spectrum (LPsrc.cpp:27-35): reduction only.
+template <class T> struct OpE1 {
+  static constexpr bool FI = false, SI = true, SO = false, INV = false, LIN = false;
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T>, c2<T> s, c2<T> &, c2<T> &,
+                               double (&acc)[1], double w) {
+    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_E1] = tot[0];
+  }
+};
+
+// ===================================================================== epilogues
+template <class T> struct EpiStore {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &, int, size_t, c2<T> y, double (&)[1]) { return y; }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Store phi' of a gradient step; the last CTA disarms the chain when the
+// step's pencil pass armed the stop (LPsrc.cpp:52 loop exit).
+template <class T> struct EpiFlow {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &, int, size_t, c2<T> y, double (&)[1]) { return y; }
+  __device__ static void fin(const KParams &p, int, const double (&)[1]) {
+    if (p.flow && p.flow[FW_PENDING]) p.flow[FW_GO] = 0;
+  }
+};
+
+// ngrad_cam epilogue (LPsrc.cpp:151-172): g = y - Tau phi - Gamma phi^2 + phi^3,
+// minus its mean (= -mean f), negated. Also sums the result squared
+// (nrmp, BasicOperators.cpp:158-164). aux0 = phi.
+template <class T> struct EpiNgrad {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&acc)[1]) {
+    const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    const T mg = -(T)scal_of(p, b)[SC_MU];
+    c2<T> o;
+    o.x = -((y.x - tau * ph.x - gam * (ph.x * ph.x) + ph.x * ph.x * ph.x) - mg);
+    o.y = -((y.y - tau * ph.y - gam * (ph.y * ph.y) + ph.y * ph.y * ph.y) - mg);
+    acc[0] += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+    return o;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    scal_of(p, b)[SC_GN2] = tot[0] * p.m.inv_n3;
+  }
+};
+
+// hv_cam epilogue (LOBPCG.cpp:136-156): y + (-Tau - 2 Gamma phi + 3 phi^2) v - mu.
+// aux0 = phi, aux1 = v.
+template <class T> struct EpiHv {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&)[1]) {
+    const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma, mu = (T)scal_of(p, b)[SC_MU];
+    return c2<T>{y.x + (-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * v.x - mu,
+                 y.y + (-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * v.y - mu};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// precond_camnew epilogue (LOBPCG.cpp:187-197): y - mu.
+template <class T> struct EpiPrecond {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t, c2<T> y, double (&)[1]) {
+    const T mu = (T)scal_of(p, b)[SC_MU];
+    return c2<T>{y.x - mu, y.y - mu};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+}  // namespace spm

@@ -1,0 +1,202 @@
+// Kernel chains of each hot-path routine for one grid size N and real type T.
+// Instantiated once per (N, T) in inst_<N>.cu; the host API reaches them
+// through the OpsTable of the context.
+#pragma once
+
+#include "blas1.cuh"
+#include "spm_internal.h"
+#include "spm_table.h"
+
+namespace spm {
+
+#define SPM_TRY(x)               \
+  do {                           \
+    int _s = (x);                \
+    if (_s != 0) return _s;      \
+  } while (0)
+
+// Sets the dynamic shared-memory limit of a kernel once per device. Tag makes
+// the "done" bits distinct per kernel (the kernels share one function type).
+template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, int dev) {
+  static unsigned done = 0;  // one bit per device (first 32)
+  if (dev < 32 && (done >> dev) & 1u) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && dev < 32) done |= 1u << dev;
+  return e;
+}
+
+template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p,
+                                                               int nb, const char *what) {
+  cudaError_t e = prepare<Tag>(kern, smem, c->device);
+  if (e != cudaSuccess) return spm_fail_cuda(e, what);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(Geo<N>::BLOCKS, nb, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = Geo<N>::CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  c->launches++;
+  e = cudaLaunchKernelEx(&cfg, kern, p);
+  return e == cudaSuccess ? 0 : spm_fail_cuda(e, what);
+}
+
+template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
+  struct Tag {};
+  return launch_cluster<Tag, N>(c, plane_fwd_kernel<N, T, Pro>, plane_smem<N, T>(), p, nb, "plane_fwd");
+}
+template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p, int nb) {
+  struct Tag {};
+  return launch_cluster<Tag, N>(c, plane_inv_kernel<N, T, Epi>, plane_smem<N, T>(), p, nb, "plane_inv");
+}
+template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p, int nb) {
+  auto kern = pencil_kernel<N, T, Op>;
+  constexpr size_t smem = pencil_smem<N, T>();
+  struct Tag {};
+  cudaError_t e = prepare<Tag>(kern, smem, c->device);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "pencil attribute");
+  c->launches++;
+  kern<<<dim3(Geo<N>::PBLOCKS, nb, 1), kThreads, smem, c->stream>>>(p);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : spm_fail_cuda(e, "pencil launch");
+}
+template <int N, class T, class F> static int reduce(spm_ctx *c, const KParams &p, int nb) {
+  constexpr size_t npairs = (size_t)N * N * N / 2;
+  constexpr int blocks = (int)((npairs + kThreads - 1) / kThreads < (size_t)kReduceBlocks
+                                   ? (npairs + kThreads - 1) / kThreads
+                                   : (size_t)kReduceBlocks);
+  c->launches++;
+  field_reduce_kernel<T, F><<<dim3(blocks, nb, 1), kThreads, 0, c->stream>>>(p, npairs);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : spm_fail_cuda(e, "reduce launch");
+}
+
+template <int N, class T> struct Impl {
+  static int fft(spm_ctx *c, const void *x, void *xhat) {
+    KParams p = spm_params(c);
+    p.in[0] = x;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProIdent<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.in[0] = spm_bufA(c, 0);
+    q.sto[0] = xhat;
+    return pencil<N, T, OpFwd<T>>(c, q, 1);
+  }
+
+  static int ifft(spm_ctx *c, const void *xhat, void *x) {
+    KParams q = spm_params(c);
+    q.st[0] = xhat;
+    q.out[0] = spm_bufB(c, 0);
+    SPM_TRY((pencil<N, T, OpInv<T>>(c, q, 1)));
+    KParams p = spm_params(c);
+    p.in[0] = spm_bufB(c, 0);
+    p.out[0] = x;
+    return plane_inv<N, T, EpiStore<T>>(c, p, 1);
+  }
+
+  // E2 -> scal[SC_E2], E1 -> scal[SC_E1]
+  static int energy(spm_ctx *c, const void *phi, const void *uhat) {
+    KParams p = spm_params(c);
+    p.in[0] = phi;
+    SPM_TRY((reduce<N, T, ProGrad<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.st[0] = uhat;
+    return pencil<N, T, OpE1<T>>(c, q, 1);
+  }
+
+  // One fused semi-implicit step, gated by the flow words.
+  static int grad_step(spm_ctx *c, void *phi, void *uhat) {
+    KParams p = spm_params(c);
+    p.flow = c->flow;
+    p.stats = c->stats;
+    p.in[0] = phi;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProGrad<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.flow = c->flow;
+    q.stats = c->stats;
+    q.in[0] = spm_bufA(c, 0);
+    q.st[0] = uhat;
+    q.sto[0] = uhat;
+    q.out[0] = spm_bufB(c, 0);
+    SPM_TRY((pencil<N, T, OpGrad<T>>(c, q, 1)));
+    KParams r = spm_params(c);
+    r.flow = c->flow;
+    r.stats = c->stats;
+    r.in[0] = spm_bufB(c, 0);
+    r.out[0] = phi;
+    return plane_inv<N, T, EpiFlow<T>>(c, r, 1);
+  }
+
+  // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
+  static int ngrad(spm_ctx *c, const void *phi, void *grad) {
+    KParams p = spm_params(c);
+    p.in[0] = phi;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProNgrad<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.in[0] = spm_bufA(c, 0);
+    q.out[0] = spm_bufB(c, 0);
+    SPM_TRY((pencil<N, T, OpGmul<T, true>>(c, q, 1)));
+    KParams r = spm_params(c);
+    r.in[0] = spm_bufB(c, 0);
+    r.aux0[0] = phi;
+    r.out[0] = grad;
+    return plane_inv<N, T, EpiNgrad<T>>(c, r, 1);
+  }
+
+  // n <= kMaxBatch Hessian-vector products sharing phi.
+  static int hv(spm_ctx *c, const void *phi, const void *const *v, void *const *hv, int n) {
+    KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
+    for (int b = 0; b < n; b++) {
+      p.in[b] = v[b];
+      p.aux0[b] = phi;
+      p.out[b] = spm_bufA(c, b);
+      q.in[b] = spm_bufA(c, b);
+      q.out[b] = spm_bufB(c, b);
+      r.in[b] = spm_bufB(c, b);
+      r.aux0[b] = phi;
+      r.aux1[b] = v[b];
+      r.out[b] = hv[b];
+    }
+    SPM_TRY((plane_fwd<N, T, ProHv<T>>(c, p, n)));
+    SPM_TRY((pencil<N, T, OpGmul<T, false>>(c, q, n)));
+    return plane_inv<N, T, EpiHv<T>>(c, r, n);
+  }
+
+  // n <= kMaxBatch preconditioner applications, in place.
+  static int precond(spm_ctx *c, void *const *w, int n) {
+    KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
+    for (int b = 0; b < n; b++) {
+      p.in[b] = w[b];
+      p.out[b] = spm_bufA(c, b);
+      q.in[b] = spm_bufA(c, b);
+      q.out[b] = spm_bufB(c, b);
+      r.in[b] = spm_bufB(c, b);
+      r.out[b] = w[b];
+    }
+    SPM_TRY((plane_fwd<N, T, ProPrecond<T>>(c, p, n)));
+    SPM_TRY((pencil<N, T, OpPrecond<T>>(c, q, n)));
+    return plane_inv<N, T, EpiPrecond<T>>(c, r, n);
+  }
+
+  // <p, q> -> scal[SC_SUM0]
+  static int dot(spm_ctx *c, const void *pp, const void *qq) {
+    KParams p = spm_params(c);
+    p.in[0] = pp;
+    p.aux0[0] = qq;
+    return reduce<N, T, ProDot<T>>(c, p, 1);
+  }
+
+  static const OpsTable *table() {
+    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &ngrad, &hv, &precond, &dot};
+    return &t;
+  }
+};
+
+}  // namespace spm

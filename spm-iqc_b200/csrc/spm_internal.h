@@ -1,0 +1,40 @@
+// Context layout and helpers shared by the host translation units of
+// libspmiqc_cuda.so (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_core.cuh"
+
+struct spm_ctx {
+  int N = 0;
+  int prec = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  spm::ModelC m{};
+  size_t field_bytes = 0;   // bytes of one real field = bytes of one packed spectrum
+  void *tw = nullptr;       // twiddle table exp(-2 pi i j/N) in the context precision
+  double *partials = nullptr;
+  unsigned *tickets = nullptr;
+  double *scal = nullptr;
+  int *flow = nullptr;
+  double *stats = nullptr;
+  int stats_cap = 0;
+  void *bufA = nullptr;     // spectral scratch, scratch_cap fields
+  void *bufB = nullptr;
+  int scratch_cap = 0;
+  double *host_scal = nullptr;  // pinned
+  int *host_flow = nullptr;     // pinned
+  uint64_t launches = 0;
+  void *extra = nullptr;        // solver state (LOBPCG / SPM work arrays)
+};
+
+int spm_fail(int status, const char *what);
+int spm_fail_cuda(cudaError_t e, const char *what);
+spm::KParams spm_params(const spm_ctx *c);
+int spm_ensure_scratch(spm_ctx *c, int nb);
+char *spm_bufA(spm_ctx *c, int b);
+char *spm_bufB(spm_ctx *c, int b);
+int spm_read_scal(spm_ctx *c, int nb);
+void spm_free_extra(spm_ctx *c);

@@ -1,0 +1,26 @@
+// Per-(grid size, precision) entry points into the kernel chains. Each
+// inst_<N>.cu translation unit provides the tables of one grid size, so the
+// sizes compile in parallel.
+#pragma once
+
+struct spm_ctx;
+
+struct OpsTable {
+  int (*fft)(spm_ctx *, const void *x, void *xhat);
+  int (*ifft)(spm_ctx *, const void *xhat, void *x);
+  int (*energy)(spm_ctx *, const void *phi, const void *uhat);
+  int (*grad_step)(spm_ctx *, void *phi, void *uhat);
+  int (*ngrad)(spm_ctx *, const void *phi, void *grad);
+  int (*hv)(spm_ctx *, const void *phi, const void *const *v, void *const *hv, int n);
+  int (*precond)(spm_ctx *, void *const *w, int n);
+  int (*dot)(spm_ctx *, const void *p, const void *q);
+};
+
+// prec: 0 = FP64, 1 = FP32
+const OpsTable *spm_table_32(int prec);
+const OpsTable *spm_table_64(int prec);
+const OpsTable *spm_table_96(int prec);
+const OpsTable *spm_table_128(int prec);
+const OpsTable *spm_table_160(int prec);
+const OpsTable *spm_table_192(int prec);
+const OpsTable *spm_table_256(int prec);

@@ -1,0 +1,197 @@
+"""Python mirror of the C ABI of libspmiqc_cuda.so (include/spmiqc.h).
+
+Method names follow the SPM-IQC routines they replace (get_Ene, get_min_u_F,
+ngrad_cam, hv_cam, precond_camnew, my_fft, my_ifft, inpfp, ...). Device memory
+comes from torch tensors (plumbing only): real fields are contiguous CUDA
+tensors of shape (N, N, N) in the context's precision, packed spectra are
+complex tensors of shape (N, N, N // 2).
+
+There is no CPU fallback: if the library is missing or no GPU is visible the
+constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libspmiqc_cuda.so")
+
+SPM_FP64, SPM_FP32 = 0, 1
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class SpmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"spmiqc status {status}: {msg}")
+        self.status = status
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("res", ctypes.c_double),
+                ("grad_norm", ctypes.c_double), ("e1", ctypes.c_double)]
+
+
+def lib():
+    """Loads libspmiqc_cuda.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built; run `python spm-iqc_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "spm_ctx_create": [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_int, _vp, ctypes.POINTER(_vp)],
+            "spm_ctx_destroy": [_vp],
+            "spm_set_stream": [_vp, _vp],
+            "spm_sync": [_vp],
+            "spm_fft": [_vp, _vp, _vp],
+            "spm_ifft": [_vp, _vp, _vp],
+            "spm_spectrum_to_full": [_vp, _vp, _vp],
+            "spm_spectrum_from_full": [_vp, _vp, _vp],
+            "spm_energy": [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
+            "spm_grad_flow": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(StepStats),
+                              ctypes.POINTER(ctypes.c_int)],
+            "spm_ngrad": [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
+            "spm_hv": [_vp, _vp, _vp, _vp, ctypes.c_int],
+            "spm_precond": [_vp, _vp, ctypes.c_int],
+            "spm_inpfp": [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
+            "spm_supported_size": [ctypes.c_int],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.spm_last_error.restype = ctypes.c_char_p
+        L.spm_status_str.restype = ctypes.c_char_p
+        L.spm_status_str.argtypes = [ctypes.c_int]
+        L.spm_field_bytes.restype = ctypes.c_size_t
+        L.spm_field_bytes.argtypes = [_vp]
+        L.spm_launch_count.restype = ctypes.c_uint64
+        L.spm_launch_count.argtypes = [_vp]
+        _lib = L
+    return _lib
+
+
+def check(status: int):
+    if status != 0:
+        raise SpmError(status, lib().spm_last_error().decode())
+
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+class SpmContext:
+    """One grid + model parameters on one CUDA device (the reference's globals)."""
+
+    def __init__(self, N: int, L: float = 26.0, Tau: float = -0.0061, Gamma: float = 0.30, dt: float = 0.3,
+                 precision: str = "fp64", stream=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("spmiqc needs a CUDA device (no CPU path)")
+        self.torch = torch
+        self.N = int(N)
+        self.L, self.Tau, self.Gamma, self.dt = float(L), float(Tau), float(Gamma), float(dt)
+        self.precision = precision
+        self.prec = SPM_FP64 if precision == "fp64" else SPM_FP32
+        self.rdtype = torch.float64 if self.prec == SPM_FP64 else torch.float32
+        self.cdtype = torch.complex128 if self.prec == SPM_FP64 else torch.complex64
+        h = _vp()
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib().spm_ctx_create(self.N, self.L, self.Tau, self.Gamma, self.dt, self.prec, _vp(s),
+                                   ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- buffers
+    def field(self, nb: int | None = None):
+        shape = (self.N,) * 3 if nb is None else (nb,) + (self.N,) * 3
+        return self.torch.zeros(shape, dtype=self.rdtype, device="cuda")
+
+    def spectrum(self):
+        return self.torch.zeros((self.N, self.N, self.N // 2), dtype=self.cdtype, device="cuda")
+
+    def launches(self) -> int:
+        return int(lib().spm_launch_count(self.h))
+
+    def sync(self):
+        check(lib().spm_sync(self.h))
+
+    # ---- My_FFT.cpp
+    def my_fft(self, x, xhat=None):
+        xhat = self.spectrum() if xhat is None else xhat
+        check(lib().spm_fft(self.h, _ptr(x), _ptr(xhat)))
+        return xhat
+
+    def my_ifft(self, xhat, x=None):
+        x = self.field() if x is None else x
+        check(lib().spm_ifft(self.h, _ptr(xhat), _ptr(x)))
+        return x
+
+    def to_full(self, xhat):
+        full = self.torch.zeros((self.N,) * 3, dtype=self.torch.complex128, device="cuda")
+        check(lib().spm_spectrum_to_full(self.h, _ptr(xhat), _ptr(full)))
+        return full
+
+    def from_full(self, full):
+        xhat = self.spectrum()
+        full = full.to(self.torch.complex128).contiguous()
+        check(lib().spm_spectrum_from_full(self.h, _ptr(full), _ptr(xhat)))
+        return xhat
+
+    # ---- LPsrc.cpp
+    def get_Ene(self, phi, uhat) -> float:
+        e = ctypes.c_double()
+        check(lib().spm_energy(self.h, _ptr(phi), _ptr(uhat), ctypes.byref(e)))
+        return e.value
+
+    def get_min_u_F(self, phi, uhat, max_steps: int, tol_grad: float = 0.0):
+        """Runs up to max_steps gradient steps in place; returns an (n, 4) array
+        of per-step (energy, res, ||grad F||, E1)."""
+        st = (StepStats * max(1, max_steps))()
+        n = ctypes.c_int()
+        check(lib().spm_grad_flow(self.h, _ptr(phi), _ptr(uhat), int(max_steps), float(tol_grad), st,
+                                  ctypes.byref(n)))
+        return np.array([[s.energy, s.res, s.grad_norm, s.e1] for s in st[:n.value]]).reshape(-1, 4)
+
+    def ngrad_cam(self, phi, grad=None):
+        grad = self.field() if grad is None else grad
+        nrm = ctypes.c_double()
+        check(lib().spm_ngrad(self.h, _ptr(phi), _ptr(grad), ctypes.byref(nrm)))
+        return grad, nrm.value
+
+    # ---- LOBPCG.cpp
+    def hv_cam(self, phi, v, hv=None):
+        """v: (N,N,N) or (nb,N,N,N); returns H v with the same shape."""
+        hv = self.torch.empty_like(v) if hv is None else hv
+        nb = 1 if v.dim() == 3 else v.shape[0]
+        check(lib().spm_hv(self.h, _ptr(phi), _ptr(v), _ptr(hv), nb))
+        return hv
+
+    def precond_camnew(self, w):
+        nb = 1 if w.dim() == 3 else w.shape[0]
+        check(lib().spm_precond(self.h, _ptr(w), nb))
+        return w
+
+    # ---- BasicOperators.cpp
+    def inpfp(self, p, q) -> float:
+        out = ctypes.c_double()
+        check(lib().spm_inpfp(self.h, _ptr(p), _ptr(q), ctypes.byref(out)))
+        return out.value
+
+    def nrmp(self, p) -> float:
+        return float(np.sqrt(self.inpfp(p, p)))

@@ -1,0 +1,113 @@
+"""CUDA path vs the FP64 oracle: transforms, energy, gradient flow, ngrad, Hv,
+preconditioner, inner products. Tolerance: the north-star FP64 bar, 1e-11
+relative (scale-relative max difference for fields)."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from oracle import spmiqc_np as npo
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [32, 64, 96, 128, 160, 192]
+TOL = 1e-11
+
+
+@pytest.fixture(scope="module")
+def spm(cuda):
+    import spmiqc
+    return spmiqc
+
+
+def t(cuda, a):
+    return cuda.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("N", SIZES + [256])
+def test_fft_matches_dft(spm, cuda, N):
+    ctx = spm.SpmContext(N)
+    x = npo.uniform_field(N, 100 + N)
+    xd = t(cuda, x)
+    xh = ctx.my_fft(xd)
+    full = ctx.to_full(xh).cpu().numpy()
+    ref = np.fft.fftn(x) / N ** 3
+    assert rel(full, ref) < 1e-13
+    back = ctx.my_ifft(xh).cpu().numpy()
+    assert rel(back, x) < 1e-13
+    # from_full is the inverse of to_full on Hermitian data
+    xh2 = ctx.from_full(cuda.from_numpy(ref).cuda())
+    assert rel(xh2.cpu().numpy(), xh.cpu().numpy()) < 1e-13
+
+
+@pytest.mark.parametrize("N", [32, 64, 96])
+def test_energy(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 7)
+    uF = m.my_fft(phi)
+    pd = t(cuda, phi)
+    uh = ctx.my_fft(pd)
+    E = ctx.get_Ene(pd, uh)
+    assert abs(E - m.energy(phi, uF)) <= TOL * abs(m.energy(phi, uF))
+
+
+@pytest.mark.parametrize("N", [32, 64, 96, 160])
+def test_grad_flow_steps(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 11)
+    pd = t(cuda, phi)
+    uh = ctx.my_fft(pd)
+    st = ctx.get_min_u_F(pd, uh, 12)
+    assert st.shape == (12, 4)
+    p, u = phi.copy(), m.my_fft(phi)
+    for s in range(12):
+        g = m.grad_norm(p)
+        p, u, e, r = m.grad_step(p, u)
+        assert abs(st[s, 0] - e) <= TOL * abs(e), s
+        assert abs(st[s, 1] - r) <= 1e-9 * abs(r), s
+        assert abs(st[s, 2] - g) <= 1e-9 * abs(g), s
+    assert rel(pd.cpu().numpy(), p) < TOL
+    assert rel(ctx.to_full(uh).cpu().numpy(), u) < TOL
+
+
+@pytest.mark.parametrize("N", [32, 64, 96])
+def test_ngrad(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 3)
+    g, nrm = ctx.ngrad_cam(t(cuda, phi))
+    ref = m.ngrad(phi)
+    assert rel(g.cpu().numpy(), ref) < TOL
+    assert abs(nrm - m.nrmp(ref)) <= TOL * m.nrmp(ref)
+
+
+@pytest.mark.parametrize("N", [32, 64, 128])
+def test_hv_batch(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 5)
+    V = np.stack([npo.uniform_field(N, 20 + i, amp=1.0) for i in range(3)])
+    H = ctx.hv_cam(t(cuda, phi), t(cuda, V)).cpu().numpy()
+    for i in range(3):
+        assert rel(H[i], m.hv(phi, V[i])) < TOL
+
+
+@pytest.mark.parametrize("N", [32, 64])
+def test_precond_batch(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    W = np.stack([npo.uniform_field(N, 40 + i, amp=1.0) for i in range(2)])
+    Wd = t(cuda, W)
+    ctx.precond_camnew(Wd)
+    out = Wd.cpu().numpy()
+    for i in range(2):
+        assert rel(out[i], m.precond(W[i])) < TOL
+
+
+def test_inpfp(spm, cuda):
+    N = 64
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    a, b = npo.uniform_field(N, 1), npo.uniform_field(N, 2)
+    assert abs(ctx.inpfp(t(cuda, a), t(cuda, b)) - m.inpfp(a, b)) <= 1e-12 * abs(m.inpfp(a, b))
