@@ -1,0 +1,353 @@
+"""Headline benchmark: semi-implicit gradient-flow steps/s on a 256^3 grid, FP64.
+
+Workload (one "step" = one get_min_u_F iteration, LPsrc.cpp:52-110, with its
+energy, res and ||grad F|| reductions): N = 256, L = 26, Tau = -0.0061,
+Gamma = 0.30, dt = 0.3, phi0 = 0.15 * sum over the 30 icosahedral shell vectors
+of cos(2 pi n.x/N + theta) + N(0, 1e-3^2) noise (seeded). Fields stay in HBM;
+each step touches 1.07 GB (> the 126 MB L2), so no L2 flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank runs an independent 256^3 flow (replicas:
+the path needs no exchange between GPUs); value = steps of all ranks / max
+rank time. Extra keys report Hv/s (batch of 8), FP32 steps/s, per-step p50/p99,
+the per-kernel roofline and the CPU baseline.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "spm-iqc_b200"))
+
+N = 256
+L, TAU, GAMMA, DT = 26.0, -0.0061, 0.30, 0.3
+METRIC = "N=256^3 grad-flow steps/s (FP64)"
+WORKLOAD = ("grad-flow 256^3 FP64, L=26, Tau=-0.0061, Gamma=0.30, dt=0.3, phi0 = icosahedral "
+            "30-vector cosine shell (amp 0.15) + N(0,1e-3) noise")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(self.idx)], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for i, n in enumerate(names):
+                    if "Active" in r[5 + i] and "Not" not in r[5 + i]:
+                        reasons.add(n)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def initial_field(seed: int):
+    import inputs
+    return inputs.cosine_shell(N, inputs.icosahedral_shell(), amp=0.15, seed=seed, noise=1e-3)
+
+
+def cpu_reference_steps(phi, budget_s: float, max_steps: int, warm: int = 1):
+    """Times the reference's own get_min_u_F loop (compiled in place, shimmed
+    FFT on all host threads), one iteration per call, until budget_s elapses."""
+    from oracle import refbind
+    threads = os.cpu_count() or 1
+    r = refbind.Ref(N, L, TAU, GAMMA, DT, threads=threads)
+    r.set_state(phi)
+    for _ in range(warm):
+        r.get_min_u_F(1)
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        r.get_min_u_F(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    r.close()
+    return n / dt, threads, n, dt
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import refbind
+    if not refbind.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspmref.so not built"}))
+        return 0
+    phi = initial_field(1)
+    warm = min(args.warmup, 1)
+    v, cores, n, dt = cpu_reference_steps(phi, budget_s=90.0, max_steps=args.steps, warm=warm)
+    sample = (f"{n} of the requested {args.steps} steps (each step the full 256^3 workload), "
+              f"{dt:.1f} s, after {warm} warm-up step(s); reference src/*.cpp compiled unchanged with the "
+              f"project FFT shim on {cores} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
+            "steps": n, "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "N": N},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--only-flow", action="store_true",
+                    help="run only the warm-up and timed gradient steps (used for ncu captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_setup()
+    if args.impl == "reference":
+        rc = reference_arm(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import numpy as np
+    import torch
+    import spmiqc
+
+    torch.cuda.set_device(local)
+    L_ = spmiqc.lib()
+    stream = torch.cuda.current_stream()
+    ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp64", stream=stream.cuda_stream)
+    phi_h = initial_field(1 + rank)
+    phi = torch.from_numpy(phi_h).cuda()
+    uh = ctx.my_fft(phi)
+    S = N ** 3 * 8
+
+    def run_steps(k, phi_t, uh_t, c=ctx):
+        spmiqc.check(L_.spm_grad_flow_enqueue(c.h, phi_t.data_ptr(), uh_t.data_ptr(), int(k), 0.0))
+
+    def collect(c=ctx):
+        n = ctypes.c_int()
+        spmiqc.check(L_.spm_grad_flow_collect(c.h, None, 0, ctypes.byref(n)))
+        return n.value
+
+    L_.spm_grad_flow_enqueue.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_double]
+    L_.spm_grad_flow_collect.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int)]
+    L_.spm_grad_step_profile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double)]
+    L_.spm_grad_flow_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+
+    # warm-up
+    run_steps(args.warmup, phi, uh)
+    assert collect() == args.warmup
+    # timed region: exactly K gated steps (the stop rule never fires on this workload; checked below)
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run_steps(args.steps, phi, uh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    launches = ctx.launches() - l0
+    done = collect()
+    if done != args.steps:
+        raise RuntimeError(f"the flow stopped after {done} of {args.steps} steps; timing would be invalid")
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    value = world * args.steps / (ms_max / 1000.0)
+    if args.only_flow:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "steps/s", "steps": args.steps,
+                              "warmup": args.warmup, "gpu_launches": int(launches), "only_flow": True}))
+        ctx.close()
+        return 0
+
+    # per-step latency distribution (event after each step)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(201)]
+    evs[0].record(stream)
+    for i in range(200):
+        run_steps(1, phi, uh)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    lat = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(200))
+    p50, p99 = lat[100], lat[197]
+
+    # per-kernel durations -> roofline of the dominant (pencil) pass
+    kms = (ctypes.c_double * 3)()
+    spmiqc.check(L_.spm_grad_step_profile(ctx.h, phi.data_ptr(), uh.data_ptr(), 50, kms))
+    kms = list(kms)
+    hbm, peak_kind = peaks()
+    kern_bytes = [2 * S, 4 * S, 2 * S]  # plane-fwd: phi in, A out; pencil: A, u in, u', B out; plane-inv: B in, phi out
+    dom = int(np.argmax(kms))
+    achieved = kern_bytes[dom] / (kms[dom] * 1e-3) / 1e9
+    step_bytes = sum(kern_bytes)
+    names = ["plane_fwd<ProGrad>", "pencil<OpGrad>", "plane_inv<EpiFlow>"]
+
+    # Hessian-vector products, block of 8 (LOBPCG k = 8)
+    V = torch.from_numpy(np.random.default_rng(5).standard_normal((8, N, N, N))).cuda()
+    HV = torch.empty_like(V)
+    ctx.hv_cam(phi, V, HV)
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    h0.record(stream)
+    for _ in range(reps):
+        ctx.hv_cam(phi, V, HV)
+    h1.record(stream)
+    torch.cuda.synchronize()
+    hv_per_s = 8 * reps / (h0.elapsed_time(h1) / 1000.0)
+    del V, HV
+
+    # FP32 bulk (same workload, FP32 transforms, FP64 reductions)
+    ctx32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
+    phi32 = torch.from_numpy(phi_h.astype(np.float32)).cuda()
+    uh32 = ctx32.my_fft(phi32)
+    run_steps(args.warmup, phi32, uh32, ctx32)
+    collect(ctx32)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    run_steps(args.steps, phi32, uh32, ctx32)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    fp32_value = args.steps / (f0.elapsed_time(f1) / 1000.0)
+    ctx32.close()
+
+    # end to end through the C ABI with the field in pinned host memory: per
+    # step, upload phi, transform, one step, download phi and the step record
+    ph_host = torch.from_numpy(phi_h.copy()).pin_memory()
+    rec = (spmiqc.StepStats * 1)()
+    nd = ctypes.c_int()
+    spmiqc.check(L_.spm_grad_flow_host(ctx.h, ph_host.data_ptr(), 1, 0.0, rec, ctypes.byref(nd)))
+    e2e_steps = 20
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        spmiqc.check(L_.spm_grad_flow_host(ctx.h, ph_host.data_ptr(), 1, 0.0, rec, ctypes.byref(nd)))
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * e2e_steps / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, cores, n, dt = cpu_reference_steps(phi_h, budget_s=20.0, max_steps=10, warm=1)
+            cpu = {"value": v, "unit": "steps/s", "cores": cores, "kind": "reference",
+                   "sample": f"{n} full 256^3 steps in {dt:.1f} s (reference src/*.cpp compiled unchanged, "
+                             f"project FFT shim on {cores} threads)"}
+        except Exception as ex:  # oracle not built on this box
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "N": N, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (1.07 GB of fields per step)"},
+            "p50_ms": p50, "p99_ms": p99,
+            "hv_per_s": hv_per_s, "fp32_steps_per_s": fp32_value,
+            "kernels_ms": dict(zip(names, kms)),
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "algorithmic_bytes": kern_bytes[dom], "traffic": None,
+                         "step_frac": (step_bytes / (ms_max / args.steps * 1e-3) / 1e9) / hbm},
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": S, "d2h_bytes_per_step": S + 32},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

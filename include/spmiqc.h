@@ -107,6 +107,25 @@ int spm_energy(spm_ctx *ctx, const void *phi, const void *uhat, double *energy);
 int spm_grad_flow(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol_grad,
                   spm_step_stats *stats, int *steps_done);
 
+/* The asynchronous form of spm_grad_flow: enqueues exactly nsteps gated steps
+ * on the context stream and returns without synchronising (the stop rule is
+ * evaluated on the device; steps after it do no work). Capturable in a CUDA
+ * graph. spm_grad_flow_collect synchronises and returns the records. */
+int spm_grad_flow_enqueue(spm_ctx *ctx, void *phi, void *uhat, int nsteps, double tol_grad);
+int spm_grad_flow_collect(spm_ctx *ctx, spm_step_stats *stats, int max_records, int *steps_done);
+
+/* get_min_u_F with the field in host memory (the reference's u_R_local,
+ * as real values): copies phi_host in, sets uhat = my_fft(phi), runs up to
+ * max_steps steps and copies phi back. phi_host holds N^3 values of the
+ * context precision (pinned memory recommended). */
+int spm_grad_flow_host(spm_ctx *ctx, void *phi_host, int max_steps, double tol_grad,
+                       spm_step_stats *stats, int *steps_done);
+
+/* Runs reps ungated gradient steps with CUDA events between the three
+ * transform passes; ms[0..2] receive the mean duration of the plane-forward,
+ * pencil and plane-inverse kernels. (Measurement aid; phi/uhat advance.) */
+int spm_grad_step_profile(spm_ctx *ctx, void *phi, void *uhat, int reps, double *ms);
+
 /* ngrad_cam (LPsrc.cpp:119-173): grad = -grad F(phi). If norm is non-NULL it
  * receives nrmp(grad) (synchronises). */
 int spm_ngrad(spm_ctx *ctx, const void *phi, void *grad, double *norm);

@@ -109,14 +109,20 @@ template <int N, class T> struct Impl {
     return pencil<N, T, OpE1<T>>(c, q, 1);
   }
 
-  // One fused semi-implicit step, gated by the flow words.
-  static int grad_step(spm_ctx *c, void *phi, void *uhat) {
+  // One fused semi-implicit step, gated by the flow words. With ev non-null,
+  // records ev[0..3] around the three passes (for per-kernel timing).
+  static int grad_step_ev(spm_ctx *c, void *phi, void *uhat, void *const *ev) {
+    auto rec = [&](int i) {
+      if (ev) cudaEventRecord((cudaEvent_t)ev[i], c->stream);
+    };
     KParams p = spm_params(c);
     p.flow = c->flow;
     p.stats = c->stats;
     p.in[0] = phi;
     p.out[0] = spm_bufA(c, 0);
+    rec(0);
     SPM_TRY((plane_fwd<N, T, ProGrad<T>>(c, p, 1)));
+    rec(1);
     KParams q = spm_params(c);
     q.flow = c->flow;
     q.stats = c->stats;
@@ -125,13 +131,17 @@ template <int N, class T> struct Impl {
     q.sto[0] = uhat;
     q.out[0] = spm_bufB(c, 0);
     SPM_TRY((pencil<N, T, OpGrad<T>>(c, q, 1)));
+    rec(2);
     KParams r = spm_params(c);
     r.flow = c->flow;
     r.stats = c->stats;
     r.in[0] = spm_bufB(c, 0);
     r.out[0] = phi;
-    return plane_inv<N, T, EpiFlow<T>>(c, r, 1);
+    SPM_TRY((plane_inv<N, T, EpiFlow<T>>(c, r, 1)));
+    rec(3);
+    return 0;
   }
+  static int grad_step(spm_ctx *c, void *phi, void *uhat) { return grad_step_ev(c, phi, uhat, nullptr); }
 
   // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
   static int ngrad(spm_ctx *c, const void *phi, void *grad) {
@@ -194,7 +204,7 @@ template <int N, class T> struct Impl {
   }
 
   static const OpsTable *table() {
-    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &ngrad, &hv, &precond, &dot};
+    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_step_ev, &ngrad, &hv, &precond, &dot};
     return &t;
   }
 };

@@ -188,6 +188,8 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
   cudaFree(c->stats);
   cudaFree(c->bufA);
   cudaFree(c->bufB);
+  cudaFree(c->host_phi);
+  cudaFree(c->host_uhat);
   if (c->host_scal) cudaFreeHost(c->host_scal);
   if (c->host_flow) cudaFreeHost(c->host_flow);
   delete c;
@@ -255,27 +257,71 @@ extern "C" int spm_energy(spm_ctx *c, const void *phi, const void *uhat, double 
   return SPM_OK;
 }
 
+static __global__ void flow_init_kernel(int *flow) {
+  flow[FW_GO] = 1;
+  flow[FW_PENDING] = 0;
+  flow[FW_ITER] = 0;
+  flow[3] = 0;
+}
+
+static int ensure_stats(spm_ctx *c, int n) {
+  if (c->stats_cap >= n) return SPM_OK;
+  if (c->stats) cudaStreamSynchronize(c->stream);
+  cudaFree(c->stats);
+  c->stats = nullptr;
+  c->stats_cap = 0;
+  const int cap = std::max(n, 1024);
+  cudaError_t e = cudaMalloc(&c->stats, sizeof(double) * 4 * (size_t)cap);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "stats buffer");
+  c->stats_cap = cap;
+  return SPM_OK;
+}
+
+extern "C" int spm_grad_flow_enqueue(spm_ctx *c, void *phi, void *uhat, int nsteps, double tol_grad) {
+  if (!c || !phi || !uhat || nsteps < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
+  SPM_TRY(spm_ensure_scratch(c, 1));
+  SPM_TRY(ensure_stats(c, nsteps));
+  c->launches++;
+  flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
+  const OpsTable *t = table_of(c);
+  c->m.tol_grad = tol_grad;
+  int rc = SPM_OK;
+  for (int i = 0; i < nsteps && rc == SPM_OK; i++) rc = t->grad_step(c, phi, uhat);
+  c->m.tol_grad = 0.0;
+  return rc;
+}
+
+extern "C" int spm_grad_flow_collect(spm_ctx *c, spm_step_stats *stats, int max_records, int *steps_done) {
+  if (!c) return spm_fail(SPM_ERR_ARG, "ctx is NULL");
+  cudaError_t e = cudaMemcpyAsync(c->host_flow, c->flow, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "grad flow");
+  const int done = c->host_flow[FW_ITER];
+  if (steps_done) *steps_done = done;
+  const int n = std::min(done, max_records);
+  if (stats && n > 0) {
+    e = cudaMemcpy(stats, c->stats, sizeof(double) * 4 * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "stats read");
+    for (int i = 0; i < n; i++)
+      if (!std::isfinite(stats[i].energy) || !std::isfinite(stats[i].grad_norm))
+        return spm_fail(SPM_ERR_NONFINITE, "non-finite energy or gradient norm");
+  }
+  return SPM_OK;
+}
+
 extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, double tol_grad,
                              spm_step_stats *stats, int *steps_done) {
   if (!c || !phi || !uhat || max_steps < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
   if (steps_done) *steps_done = 0;
   if (max_steps == 0) return SPM_OK;
   SPM_TRY(spm_ensure_scratch(c, 1));
-  if (c->stats_cap < max_steps) {
-    cudaFree(c->stats);
-    c->stats = nullptr;
-    c->stats_cap = 0;
-    cudaError_t e = cudaMalloc(&c->stats, sizeof(double) * 4 * (size_t)max_steps);
-    if (e != cudaSuccess) return spm_fail_cuda(e, "stats buffer");
-    c->stats_cap = max_steps;
-  }
-  c->m.tol_grad = tol_grad;
-  static const int init[4] = {1, 0, 0, 0};
-  std::memcpy(c->host_flow, init, sizeof(init));
-  cudaError_t e = cudaMemcpyAsync(c->flow, c->host_flow, sizeof(init), cudaMemcpyHostToDevice, c->stream);
-  if (e != cudaSuccess) return spm_fail_cuda(e, "flow init");
+  SPM_TRY(ensure_stats(c, max_steps));
+  c->launches++;
+  flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
   const OpsTable *t = table_of(c);
+  c->m.tol_grad = tol_grad;
   int enq = 0, chunk = 8, rc = SPM_OK;
+  cudaError_t e = cudaSuccess;
   while (enq < max_steps) {
     const int n = std::min(chunk, max_steps - enq);
     for (int i = 0; i < n && rc == SPM_OK; i++) rc = t->grad_step(c, phi, uhat);
@@ -289,16 +335,51 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
   }
   c->m.tol_grad = 0.0;
   if (rc != SPM_OK) return rc;
-  const int done = c->host_flow[FW_ITER];
-  if (steps_done) *steps_done = done;
-  if (stats && done > 0) {
-    e = cudaMemcpy(stats, c->stats, sizeof(double) * 4 * (size_t)done, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return spm_fail_cuda(e, "stats read");
-    for (int i = 0; i < done; i++)
-      if (!std::isfinite(stats[i].energy) || !std::isfinite(stats[i].grad_norm))
-        return spm_fail(SPM_ERR_NONFINITE, "non-finite energy or gradient norm");
+  return spm_grad_flow_collect(c, stats, max_steps, steps_done);
+}
+
+extern "C" int spm_grad_flow_host(spm_ctx *c, void *phi_host, int max_steps, double tol_grad,
+                                  spm_step_stats *stats, int *steps_done) {
+  if (!c || !phi_host || max_steps < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (!c->host_phi) {
+    cudaError_t e = cudaMalloc(&c->host_phi, c->field_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->host_uhat, c->field_bytes);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "host-path buffers");
   }
-  return SPM_OK;
+  cudaError_t e = cudaMemcpyAsync(c->host_phi, phi_host, c->field_bytes, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "phi upload");
+  SPM_TRY(spm_fft(c, c->host_phi, c->host_uhat));
+  SPM_TRY(spm_grad_flow(c, c->host_phi, c->host_uhat, max_steps, tol_grad, stats, steps_done));
+  e = cudaMemcpyAsync(phi_host, c->host_phi, c->field_bytes, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "phi download");
+}
+
+extern "C" int spm_grad_step_profile(spm_ctx *c, void *phi, void *uhat, int reps, double *ms) {
+  if (!c || !phi || !uhat || !ms || reps < 1) return spm_fail(SPM_ERR_ARG, "bad argument");
+  SPM_TRY(spm_ensure_scratch(c, 1));
+  SPM_TRY(ensure_stats(c, reps));
+  c->launches++;
+  flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
+  cudaEvent_t ev[4];
+  for (int i = 0; i < 4; i++) cudaEventCreate(&ev[i]);
+  double acc[3] = {0, 0, 0};
+  int rc = SPM_OK;
+  const OpsTable *t = table_of(c);
+  for (int r = 0; r < reps && rc == SPM_OK; r++) {
+    rc = t->grad_step_ev(c, phi, uhat, (void *const *)ev);
+    if (rc != SPM_OK) break;
+    cudaError_t e = cudaEventSynchronize(ev[3]);
+    if (e != cudaSuccess) { rc = spm_fail_cuda(e, "profile"); break; }
+    for (int k = 0; k < 3; k++) {
+      float f = 0;
+      cudaEventElapsedTime(&f, ev[k], ev[k + 1]);
+      acc[k] += f;
+    }
+  }
+  for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
+  for (int k = 0; k < 3; k++) ms[k] = acc[k] / reps;
+  return rc;
 }
 
 extern "C" int spm_ngrad(spm_ctx *c, const void *phi, void *grad, double *norm) {

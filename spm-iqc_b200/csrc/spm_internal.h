@@ -28,6 +28,8 @@ struct spm_ctx {
   int *host_flow = nullptr;     // pinned
   uint64_t launches = 0;
   void *extra = nullptr;        // solver state (LOBPCG / SPM work arrays)
+  void *host_phi = nullptr;     // device copies used by the host-buffer entry points
+  void *host_uhat = nullptr;
 };
 
 int spm_fail(int status, const char *what);
