@@ -142,6 +142,21 @@ int spm_precond(spm_ctx *ctx, void *w, int nb);
 /* inpfp (BasicOperators.cpp:132-143): <p, q> = (1/N^3) sum p q. */
 int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
 
+/* Allocation-free batch of inner products; no counterpart in the reference.
+ * For callers that cannot allocate device memory when they need the result
+ * (their device memory is fully reserved by their own pool, or a cudaMalloc's
+ * implicit synchronisation would stall their other streams): needs no context
+ * and allocates nothing. out[b] = (1/n) sum_i p[b*n + i] * q[b*n + i] for
+ * b < nb, with p, q device arrays of nb*n values (double for SPM_FP64, float
+ * for SPM_FP32) and out a device array of nb doubles, enqueued on stream.
+ * nb is limited to 16 (SPM_ERR_ARG above): the reduction's scratch is a fixed
+ * ~77 KB array in the library's device memory, resident on every device that
+ * loads the library until exit. Calls share that array: calls that overlap on
+ * the GPU race and must be ordered. The first call on a device looks up the
+ * array's address; make it before any stream capture begins. */
+int spm_inpfp_batch_noalloc(size_t n, int nb, int precision, const void *p, const void *q,
+                            double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
