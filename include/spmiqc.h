@@ -137,6 +137,40 @@ int spm_hv(spm_ctx *ctx, const void *phi, const void *v, void *hv, int nb);
 /* precond_camnew (LOBPCG.cpp:168-199), in place on nb vectors. */
 int spm_precond(spm_ctx *ctx, void *w, int nb);
 
+/* --------------------------------------------------------------- LOBPCG */
+
+/* hiosd_lobpcg_initialization (LOBPCG.cpp:10-109): V (k fields, 1 <= k <= 8)
+ * receives a random start block -- Eigen's unseeded MatrixXd::Random(k, N^3)
+ * replaced by a SplitMix64 stream, V[i][j] = -1 + 2 u(seed, j*k + i) --, each
+ * vector minus its mean, then Gram-Schmidt orthonormalised under inpfp. */
+int spm_lobpcg_init(spm_ctx *ctx, void *V, int k, uint64_t seed);
+
+/* hiosd_lobpcg_inip (LOBPCG.cpp:207-487): one call of maxiter LOBPCG
+ * iterations for the k lowest eigenpairs of H(phi), updating V (k fields) in
+ * place. Each iteration builds [V, W, P] with the reference's order and 1e-8
+ * dropping rule and solves the Rayleigh-Ritz problem; block inner products
+ * run on the FP64 tensor cores. If tol > 0 the call also stops when every
+ * residual ||H v_i - lambda_i v_i|| is <= tol. On return evals[i] =
+ * <v_i, H v_i> and resid[i] the residual of the returned block (host arrays
+ * of k, may be NULL), *iters the iterations done. */
+int spm_lobpcg(spm_ctx *ctx, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
+               double *resid, int *iters);
+
+/* ------------------------------------------------------------------ SPM */
+
+/* get_Tv (SPM.cpp:15-32): v = (phi1 - phi0) / nrmp(phi1 - phi0). */
+int spm_get_tv(spm_ctx *ctx, const void *phi0, const void *phi1, void *v);
+/* Natural_Forces (SPM.cpp:34-99) and MinMax_Forces (SPM.cpp:103-168): one
+ * semi-implicit force step on x in place along the unit tangent v. */
+int spm_natural_forces(spm_ctx *ctx, void *x, const void *v);
+int spm_minmax_forces(spm_ctx *ctx, void *x, const void *v);
+/* Spring_Pairing (SPM.cpp:170-263) on the replica pair (phi0, phi1) in place:
+ * up to maxiter iterations while res = max_i nrmp(ngrad(phi_i)) > tol.
+ * res_hist (host, may be NULL, >= maxiter entries) receives res per
+ * iteration; *iters the iterations done. */
+int spm_spring_pairing(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double *res_hist,
+                       int *iters);
+
 /* ------------------------------------------------------------ BLAS-1 */
 
 /* inpfp (BasicOperators.cpp:132-143): <p, q> = (1/N^3) sum p q. */

@@ -42,6 +42,19 @@ template <class T> struct ProDot {
   }
 };
 
+// Field mean (mean_Cplx, BasicOperators.cpp:121-130): scal[SC_SUM0] = sum / N^3.
+template <class T> struct ProSum {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &, int, size_t, c2<T> x, double (&acc)[1]) {
+    acc[0] += (double)x.x + (double)x.y;
+    return x;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    p.scal[(size_t)b * kScal + SC_SUM0] = tot[0] * p.m.inv_n3;
+  }
+};
+
 // Packed spectrum -> the reference's full complex spectrum (double, interleaved).
 template <class T>
 __global__ void packed_to_full_kernel(const c2<T> *__restrict__ pk, double2 *__restrict__ full, int N) {

@@ -1,0 +1,190 @@
+// Block kernels of the LOBPCG and SPM solvers: the tall-skinny Gram on FP64
+// tensor cores, the block combination Y = X C + d, the seeded start block, and
+// the SPM spring update / stop check.
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace spm {
+
+constexpr int kBlkMax = 24;      // vectors per block operand (3k with k <= 8)
+constexpr int kGramBlocks = 296; // 2 CTAs per SM
+constexpr int kGramWarps = 8;
+
+struct GramP {
+  const void *X[kBlkMax];
+  const void *Y[kBlkMax];
+  int ma, mb;
+  size_t n;          // points per vector (multiple of 4)
+  double inv_n;      // normalisation of <.,.> (1/N^3)
+  double *partials;  // [kGramBlocks][kBlkMax * kBlkMax]
+  unsigned *ticket;
+  double *out;       // ma x mb, row-major
+  const int *flow;   // optional gate
+};
+
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// G[a][b] = inv_n * sum_i X_a[i] Y_b[i] for a < ma, b < mb (the Gram of
+// LOBPCG.cpp:343-358 and the inner products of the block orthogonalisations).
+// Each warp owns interleaved 4-point k-steps and accumulates the (ma x mb)
+// product in 8x8 FP64 MMA tiles; CTA and grid totals are summed in a fixed
+// order, so the result does not depend on scheduling.
+template <class T>
+__global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_constant__ GramP p) {
+  __shared__ int s_last;
+  if (p.flow && *((volatile const int *)p.flow) == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int TA = (p.ma + 7) >> 3, TB = (p.mb + 7) >> 3;
+  double acc[3][3][2];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const T *xr[3], *yr[3];
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int ra = t * 8 + gid, rb = t * 8 + gid;
+    xr[t] = (t < TA && ra < p.ma) ? reinterpret_cast<const T *>(p.X[ra]) : nullptr;
+    yr[t] = (t < TB && rb < p.mb) ? reinterpret_cast<const T *>(p.Y[rb]) : nullptr;
+  }
+  const size_t steps = p.n / 4;
+  const size_t gw = (size_t)blockIdx.x * kGramWarps + warp, W = (size_t)gridDim.x * kGramWarps;
+  for (size_t s = gw; s < steps; s += W) {
+    const size_t k = 4 * s + tig;
+    double a[3], b[3];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      a[t] = xr[t] ? (double)__ldg(xr[t] + k) : 0.0;
+      b[t] = yr[t] ? (double)__ldg(yr[t] + k) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        if (i < TA && j < TB) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  }
+  // CTA total in a fixed warp order: warp w writes its tiles, warp 0 sums
+  __shared__ double tile[kGramWarps][kBlkMax * kBlkMax];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      if (i < TA && j < TB) {
+        const int r = i * 8 + gid, c = j * 8 + 2 * tig;
+        tile[warp][r * kBlkMax + c] = acc[i][j][0];
+        tile[warp][r * kBlkMax + c + 1] = acc[i][j][1];
+      }
+  __syncthreads();
+  double *part = p.partials + (size_t)blockIdx.x * kBlkMax * kBlkMax;
+  for (int e = threadIdx.x; e < kBlkMax * kBlkMax; e += blockDim.x) {
+    const int r = e / kBlkMax, c = e % kBlkMax;
+    if (r < TA * 8 && c < TB * 8) {
+      double s = 0.0;
+      for (int w = 0; w < kGramWarps; w++) s += tile[w][e];
+      part[e] = s;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(p.ticket, 1u) == gridDim.x - 1u);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int e = threadIdx.x; e < p.ma * p.mb; e += blockDim.x) {
+    const int r = e / p.mb, c = e % p.mb;
+    double s = 0.0;
+    for (unsigned bk = 0; bk < gridDim.x; bk++) s += __ldcg(p.partials + (size_t)bk * kBlkMax * kBlkMax + r * kBlkMax + c);
+    p.out[e] = s * p.inv_n;
+  }
+  if (threadIdx.x == 0) *p.ticket = 0u;
+}
+
+struct CombP {
+  const void *X[kBlkMax + 8];
+  void *Y[kBlkMax];
+  int nin, nout;
+  size_t n;
+  const double *C;   // nin x nout, row-major: Y_q += C[p*nout + q] X_p
+  const double *d;   // nout constants or null
+  int accumulate;    // Y_q = (accumulate ? Y_q : 0) + ...
+  const int *flow;
+};
+
+// Y_q[i] = (accumulate ? Y_q[i] : 0) + sum_p C[p][q] X_p[i] + d[q]. A point's
+// inputs are all read before its outputs are written, so Y may alias X.
+template <class T>
+__global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ CombP p) {
+  __shared__ double sc[(kBlkMax + 8) * kBlkMax + kBlkMax];
+  if (p.flow && *((volatile const int *)p.flow) == 0) return;
+  for (int e = threadIdx.x; e < p.nin * p.nout; e += blockDim.x) sc[e] = p.C[e];
+  for (int e = threadIdx.x; e < p.nout; e += blockDim.x) sc[(kBlkMax + 8) * kBlkMax + e] = p.d ? p.d[e] : 0.0;
+  __syncthreads();
+  const double *dd = sc + (kBlkMax + 8) * kBlkMax;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (size_t)gridDim.x * blockDim.x) {
+    double x[kBlkMax + 8];
+#pragma unroll
+    for (int q = 0; q < kBlkMax + 8; q++) x[q] = (q < p.nin) ? (double)reinterpret_cast<const T *>(p.X[q])[i] : 0.0;
+#pragma unroll 1
+    for (int q = 0; q < p.nout; q++) {
+      T *yq = reinterpret_cast<T *>(p.Y[q]);
+      double s = p.accumulate ? (double)yq[i] : 0.0;
+#pragma unroll
+      for (int r = 0; r < kBlkMax + 8; r++)
+        if (r < p.nin) s += sc[r * p.nout + q] * x[r];
+      yq[i] = (T)(s + dd[q]);
+    }
+  }
+}
+
+// Start block of hiosd_lobpcg_initialization (LOBPCG.cpp:31-42) with
+// Eigen's MatrixXd::Random(k, N^3) replaced by a SplitMix64 stream:
+// V[i][j] = -1 + 2 u(seed, j*k + i) (the matrix is column-major).
+template <class T>
+__global__ void lobpcg_random_kernel(T *V, int k, size_t n, unsigned long long seed) {
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (size_t)gridDim.x * blockDim.x)
+    for (int i = 0; i < k; i++) {
+      unsigned long long z = seed + ((unsigned long long)(j * k + i) + 1ull) * 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z = z ^ (z >> 31);
+      const double u = (double)(z >> 11) * 1.1102230246251565404e-16;  // 2^-53
+      V[(size_t)i * n + j] = (T)(-1.0 + 2.0 * u);
+    }
+}
+
+// The two spring updates of Spring_Pairing (SPM.cpp:203-216), in the
+// reference's sequential order: phi1 sees the updated phi0.
+template <class T>
+__global__ void spring_kernel(T *phi0, T *phi1, size_t n, double dt, double ks, const int *flow) {
+  if (flow && *((volatile const int *)flow) == 0) return;
+  const T k = (T)ks, t = (T)dt;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    T p0 = phi0[i], p1 = phi1[i];
+    T fs = k * p1 + (-k) * p0;
+    p0 = (T)1 * p0 + t * fs;
+    fs = k * p0 + (-k) * p1;
+    p1 = (T)1 * p1 + t * fs;
+    phi0[i] = p0;
+    phi1[i] = p1;
+  }
+}
+
+// End of one Spring_Pairing iteration (SPM.cpp:220-256): res = max_i ||grad F(Phi_i)||
+// from the two ngrad norms, record it and disarm the chain when res <= tol.
+__global__ void spm_check_kernel(double *scal, int *flow, double *stats, double tol, int cap) {
+  if (flow[FW_GO] == 0) return;
+  const double r0 = sqrt(scal[0 * kScal + SC_GN2]), r1 = sqrt(scal[1 * kScal + SC_GN2]);
+  const double res = r0 > r1 ? r0 : r1;
+  const int it = flow[FW_ITER];
+  if (stats && it < cap) stats[it] = res;
+  flow[FW_ITER] = it + 1;
+  if (!(res > tol)) flow[FW_GO] = 0;
+}
+
+}  // namespace spm

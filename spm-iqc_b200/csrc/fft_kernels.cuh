@@ -492,11 +492,13 @@ __global__ void __launch_bounds__(kThreads) plane_inv_kernel(const __grid_consta
         for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
         Dft<+1, 8, T2>::run(u);
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
-        T2 *dst = reinterpret_cast<T2 *>(reinterpret_cast<T *>(p.out[b]) + rowoff);
+        T *outb = reinterpret_cast<T *>(p.out[b]);  // null: reductions only
+        T2 *dst = reinterpret_cast<T2 *>(outb + rowoff);
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) {
           const int j = k1 + N1 * k2;
-          dst[j] = Epi::epi(p, b, rowoff + 2 * j, u[k2], acc);
+          const T2 val = Epi::epi(p, b, rowoff + 2 * j, u[k2], acc);
+          if (outb) dst[j] = val;
         }
       }
     }

@@ -127,7 +127,7 @@ template <class T> struct ProTangent {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
   __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[1]) {
-    const c2<T> a = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const c2<T> a = p.aux0[b] ? __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx)) : c2<T>{0, 0};
     const c2<T> d = {x.x - a.x, x.y - a.y};
     acc[0] += (double)d.x * (double)d.x + (double)d.y * (double)d.y;
     return d;
@@ -261,14 +261,15 @@ template <class T> struct OpForce {
 };
 
 // Tangent spectrum v^ = FFT(d) / (N^3 ||d||) (stored) and the G-weighted
-// field Gv = IFFT(G v^, k = 0 removed) (inverse output).
-template <class T> struct OpTangent {
+// field Gv = IFFT(G v^, k = 0 removed) (inverse output). With NORM false the
+// field is taken as given (||d|| := 1), for force steps along a caller's v.
+template <class T, bool NORM = true> struct OpTangent {
   static constexpr bool FI = true, SI = false, SO = true, INV = true, LIN = false;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
   __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &so,
                                c2<T> &inv, double (&)[1], double) {
-    const T inrm = (T)(1.0 / sqrt(scal_of(p, b)[SC_NRM2]));
+    const T inrm = NORM ? (T)(1.0 / sqrt(scal_of(p, b)[SC_NRM2])) : (T)1;
     const c2<T> v = cscale(cscale(f, (T)p.m.inv_n3), inrm);
     so = v;
     const T g = (T)gk_of(Kx, Ky, Kz, p.m.invL);
@@ -343,6 +344,24 @@ template <class T> struct EpiHv {
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma, mu = (T)scal_of(p, b)[SC_MU];
     return c2<T>{y.x + (-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * v.x - mu,
                  y.y + (-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * v.y - mu};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// Tangent epilogue: returns Gv and, when p.sto[b] is set, also writes the
+// real-space tangent v = (Phi1 - Phi0) / ||Phi1 - Phi0|| (SPM.cpp:21-31) there
+// (aux0 = Phi0, aux1 = Phi1).
+template <class T> struct EpiTangent {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&)[1]) {
+    if (p.sto[b]) {
+      const c2<T> a = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+      const c2<T> c = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
+      const T d = (T)sqrt(scal_of(p, b)[SC_NRM2]);
+      *reinterpret_cast<c2<T> *>(reinterpret_cast<T *>(p.sto[b]) + idx) = c2<T>{(c.x - a.x) / d, (c.y - a.y) / d};
+    }
+    return y;
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
 };

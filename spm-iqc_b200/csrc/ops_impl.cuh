@@ -203,8 +203,73 @@ template <int N, class T> struct Impl {
     return reduce<N, T, ProDot<T>>(c, p, 1);
   }
 
+  // Tangent preparation (get_Tv, SPM.cpp:15-32, plus what the force steps
+  // need): with phi0 set, d = phi1 - phi0 is normalised and v = d/||d|| is
+  // written to v_out; with phi0 null, phi1 is the tangent as given. Always
+  // writes vhat = FFT(v)/N^3 (packed) and Gv = IFFT(G vhat, k = 0 removed).
+  static int tangent(spm_ctx *c, const void *phi0, const void *phi1, void *v_out, void *vhat, void *gv) {
+    KParams p = spm_params(c);
+    p.in[0] = phi1;
+    p.aux0[0] = phi0;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProTangent<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.in[0] = spm_bufA(c, 0);
+    q.sto[0] = vhat;
+    q.out[0] = spm_bufB(c, 0);
+    if (phi0) SPM_TRY((pencil<N, T, OpTangent<T, true>>(c, q, 1)));
+    else SPM_TRY((pencil<N, T, OpTangent<T, false>>(c, q, 1)));
+    KParams r = spm_params(c);
+    r.in[0] = spm_bufB(c, 0);
+    r.aux0[0] = phi0;
+    r.aux1[0] = phi1;
+    r.sto[0] = phi0 ? v_out : nullptr;
+    r.out[0] = gv;
+    return plane_inv<N, T, EpiTangent<T>>(c, r, 1);
+  }
+
+  // Natural_Forces (factor 1) / MinMax_Forces (factor 2) on n fields in place,
+  // all along the tangent (v, vhat, Gv) from tangent().
+  static int force(spm_ctx *c, void *const *x, int n, const void *v, const void *vhat, const void *gv,
+                   double factor) {
+    KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
+    p.m.factor = factor;
+    for (int b = 0; b < n; b++) {
+      p.in[b] = x[b];
+      p.aux0[b] = v;
+      p.aux1[b] = gv;
+      p.out[b] = spm_bufA(c, b);
+      q.in[b] = spm_bufA(c, b);
+      q.st[b] = vhat;
+      q.out[b] = spm_bufB(c, b);
+      r.in[b] = spm_bufB(c, b);
+      r.out[b] = x[b];
+    }
+    SPM_TRY((plane_fwd<N, T, ProForce<T>>(c, p, n)));
+    SPM_TRY((pencil<N, T, OpForce<T>>(c, q, n)));
+    return plane_inv<N, T, EpiStore<T>>(c, r, n);
+  }
+
+  // ||ngrad(x_b)||^2 -> scal[b][SC_GN2] without storing the gradient.
+  static int gnorm(spm_ctx *c, const void *const *x, int n) {
+    KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
+    for (int b = 0; b < n; b++) {
+      p.in[b] = x[b];
+      p.out[b] = spm_bufA(c, b);
+      q.in[b] = spm_bufA(c, b);
+      q.out[b] = spm_bufB(c, b);
+      r.in[b] = spm_bufB(c, b);
+      r.aux0[b] = x[b];
+      r.out[b] = nullptr;
+    }
+    SPM_TRY((plane_fwd<N, T, ProNgrad<T>>(c, p, n)));
+    SPM_TRY((pencil<N, T, OpGmul<T, true>>(c, q, n)));
+    return plane_inv<N, T, EpiNgrad<T>>(c, r, n);
+  }
+
   static const OpsTable *table() {
-    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_step_ev, &ngrad, &hv, &precond, &dot};
+    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_step_ev, &ngrad, &hv, &precond, &dot,
+                               &tangent, &force, &gnorm};
     return &t;
   }
 };

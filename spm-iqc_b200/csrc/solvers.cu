@@ -1,4 +1,575 @@
-// Host-side solvers built on the transform kernels (filled in below).
-#include "spm_internal.h"
+// Host-driven solvers on the transform kernels:
+//  * LOBPCG for the lowest Hessian eigenpairs (hiosd_lobpcg_initialization /
+//    hiosd_lobpcg_inip, LOBPCG.cpp:10-109, 207-487);
+//  * the Spring Pair Method (get_Tv, Natural_Forces, MinMax_Forces,
+//    Spring_Pairing, SPM.cpp:15-263).
+// Fields stay on the device. Block inner products run on the FP64 tensor cores
+// (gram_kernel); the small dense algebra (Cholesky, the Rayleigh-Ritz
+// eigenproblem of size <= 3k) runs on the host in FP64.
+#include <cuda_runtime.h>
 
-void spm_free_extra(spm_ctx *c) { (void)c; }
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/spmiqc.h"
+#include "blas1.cuh"
+#include "blockops.cuh"
+#include "spm_internal.h"
+#include "spm_table.h"
+
+using namespace spm;
+
+#define SPM_TRY(x)                 \
+  do {                             \
+    int _s = (x);                  \
+    if (_s != SPM_OK) return _s;   \
+  } while (0)
+
+namespace {
+
+struct Solver {
+  double *gram_part = nullptr;  // [kGramBlocks][kBlkMax^2]
+  unsigned *gram_ticket = nullptr;
+  double *gram_out = nullptr;   // kBlkMax^2
+  double *coef = nullptr;       // (kBlkMax + 8) * kBlkMax + kBlkMax
+  double *h_gram = nullptr;     // pinned
+  void *lob = nullptr;          // LOBPCG work fields: U, W, Y, P, Up, Vn (k each)
+  int lob_k = 0;
+  void *spm = nullptr;          // SPM: v, vhat, Gv
+  double *spm_stats = nullptr;
+  int spm_cap = 0;
+};
+
+Solver *solver(spm_ctx *c) {
+  if (!c->extra) c->extra = new Solver();
+  return reinterpret_cast<Solver *>(c->extra);
+}
+
+int ensure_base(spm_ctx *c) {
+  Solver *s = solver(c);
+  if (s->gram_part) return SPM_OK;
+  cudaError_t e = cudaMalloc(&s->gram_part, sizeof(double) * kGramBlocks * kBlkMax * kBlkMax);
+  if (e == cudaSuccess) e = cudaMalloc(&s->gram_ticket, sizeof(unsigned) * 4);
+  if (e == cudaSuccess) e = cudaMemset(s->gram_ticket, 0, sizeof(unsigned) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->gram_out, sizeof(double) * kBlkMax * kBlkMax);
+  if (e == cudaSuccess) e = cudaMalloc(&s->coef, sizeof(double) * ((kBlkMax + 8) * kBlkMax + kBlkMax));
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_gram, sizeof(double) * kBlkMax * kBlkMax);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "solver buffers");
+  return SPM_OK;
+}
+
+inline size_t npts(const spm_ctx *c) { return (size_t)c->N * c->N * c->N; }
+inline void *fld(const spm_ctx *c, void *base, int i) { return (char *)base + c->field_bytes * (size_t)i; }
+
+// G = X^T Y / N^3 (ma x mb, row-major) into host memory (synchronises).
+int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector<double> &G) {
+  Solver *s = solver(c);
+  GramP p;
+  std::memset(&p, 0, sizeof(p));
+  for (int i = 0; i < ma; i++) p.X[i] = X[i];
+  for (int i = 0; i < mb; i++) p.Y[i] = Y[i];
+  p.ma = ma;
+  p.mb = mb;
+  p.n = npts(c);
+  p.inv_n = c->m.inv_n3;
+  p.partials = s->gram_part;
+  p.ticket = s->gram_ticket;
+  p.out = s->gram_out;
+  c->launches++;
+  if (c->prec == SPM_FP64) gram_kernel<double><<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
+  else gram_kernel<float><<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->h_gram, s->gram_out, sizeof(double) * ma * mb, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "gram");
+  G.assign(s->h_gram, s->h_gram + ma * mb);
+  for (double v : G)
+    if (!std::isfinite(v)) return spm_fail(SPM_ERR_NONFINITE, "non-finite Gram entry");
+  return SPM_OK;
+}
+
+// Y_q = (acc ? Y_q : 0) + sum_p C[p*nout + q] X_p + d[q]
+int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const std::vector<double> &C,
+            const std::vector<double> *d, bool acc) {
+  Solver *s = solver(c);
+  if (nin > kBlkMax + 8 || nout > kBlkMax) return spm_fail(SPM_ERR_ARG, "combine size");
+  std::vector<double> buf((size_t)nin * nout + nout, 0.0);
+  std::copy(C.begin(), C.begin() + (size_t)nin * nout, buf.begin());
+  if (d) std::copy(d->begin(), d->begin() + nout, buf.begin() + (size_t)nin * nout);
+  // pageable source: the copy has consumed buf when the call returns
+  cudaError_t e = cudaMemcpyAsync(s->coef, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice,
+                                  c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "combine coefficients");
+  CombP p;
+  std::memset(&p, 0, sizeof(p));
+  for (int i = 0; i < nin; i++) p.X[i] = X[i];
+  for (int i = 0; i < nout; i++) p.Y[i] = Y[i];
+  p.nin = nin;
+  p.nout = nout;
+  p.n = npts(c);
+  p.C = s->coef;
+  p.d = d ? s->coef + (size_t)nin * nout : nullptr;
+  p.accumulate = acc ? 1 : 0;
+  c->launches++;
+  if (c->prec == SPM_FP64) combine_kernel<double><<<1184, 256, 0, c->stream>>>(p);
+  else combine_kernel<float><<<1184, 256, 0, c->stream>>>(p);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "combine launch");
+}
+
+// Means of n fields (mean_Cplx, BasicOperators.cpp:121-130) into host memory.
+int means(spm_ctx *c, void *const *X, int n, std::vector<double> &out) {
+  out.assign(n, 0.0);
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    const int nb = std::min(kMaxBatch, n - b0);
+    KParams p = spm_params(c);
+    for (int b = 0; b < nb; b++) p.in[b] = X[b0 + b];
+    const size_t npairs = npts(c) / 2;
+    c->launches++;
+    if (c->prec == SPM_FP64)
+      field_reduce_kernel<double, ProSum<double>><<<dim3(kReduceBlocks, nb), kThreads, 0, c->stream>>>(p, npairs);
+    else
+      field_reduce_kernel<float, ProSum<float>><<<dim3(kReduceBlocks, nb), kThreads, 0, c->stream>>>(p, npairs);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return spm_fail_cuda(e, "mean launch");
+    SPM_TRY(spm_read_scal(c, nb));
+    for (int b = 0; b < nb; b++) out[b0 + b] = c->host_scal[b * kScal + SC_SUM0];
+  }
+  return SPM_OK;
+}
+
+int hv_many(spm_ctx *c, const void *phi, void *const *v, void *const *hv, int n) {
+  const OpsTable *t = spm_table_of(c);
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    const int nb = std::min(kMaxBatch, n - b0);
+    SPM_TRY(spm_ensure_scratch(c, nb));
+    SPM_TRY(t->hv(c, phi, (const void *const *)(v + b0), hv + b0, nb));
+  }
+  return SPM_OK;
+}
+
+int precond_many(spm_ctx *c, void *const *w, int n) {
+  const OpsTable *t = spm_table_of(c);
+  for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
+    const int nb = std::min(kMaxBatch, n - b0);
+    SPM_TRY(spm_ensure_scratch(c, nb));
+    SPM_TRY(t->precond(c, w + b0, nb));
+  }
+  return SPM_OK;
+}
+
+// --------------------------------------------------------------- small algebra
+// Gram-Schmidt in the metric G (Cholesky with column dropping): column j is
+// dropped when its norm orthogonal to the kept columns before it is <= thr
+// (the nrmW / nrmVpi > 1e-8 tests of LOBPCG.cpp:298, 319). Returns the
+// coefficients B (k x k, row-major, B[p*k + q]) with X_new_q = sum_p B[p][q] X_p,
+// orthonormal for kept columns and zero for dropped ones.
+void gs_coefficients(const std::vector<double> &G, int k, double thr, std::vector<int> &keep,
+                     std::vector<double> &B) {
+  std::vector<double> R((size_t)k * k, 0.0);
+  for (int j = 0; j < k; j++) {
+    if (!keep[j]) continue;
+    double r2 = G[(size_t)j * k + j];
+    for (int i = 0; i < j; i++) {
+      if (!keep[i]) continue;
+      double s = G[(size_t)i * k + j];
+      for (int l = 0; l < i; l++)
+        if (keep[l]) s -= R[(size_t)l * k + i] * R[(size_t)l * k + j];
+      R[(size_t)i * k + j] = s / R[(size_t)i * k + i];
+      r2 -= R[(size_t)i * k + j] * R[(size_t)i * k + j];
+    }
+    if (!(r2 > thr * thr)) {
+      keep[j] = 0;
+      continue;
+    }
+    R[(size_t)j * k + j] = std::sqrt(r2);
+  }
+  // B = R^{-1} on the kept index set (upper triangular back-substitution)
+  B.assign((size_t)k * k, 0.0);
+  for (int q = 0; q < k; q++) {
+    if (!keep[q]) continue;
+    B[(size_t)q * k + q] = 1.0 / R[(size_t)q * k + q];
+    for (int p = q - 1; p >= 0; p--) {
+      if (!keep[p]) continue;
+      double s = 0.0;
+      for (int l = p + 1; l <= q; l++)
+        if (keep[l]) s += R[(size_t)p * k + l] * B[(size_t)l * k + q];
+      B[(size_t)p * k + q] = -s / R[(size_t)p * k + p];
+    }
+  }
+}
+
+// Symmetric eigenproblem by cyclic Jacobi; eigenvalues ascending, vectors as
+// columns of V (row-major n x n). Replaces Eigen's EigenSolver on the
+// symmetrised Rayleigh-Ritz matrix (LOBPCG.cpp:357-382), whose spectrum is real.
+void sym_eig(std::vector<double> A, int n, std::vector<double> &vals, std::vector<double> &V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        tot += a(i, j) * a(i, j);
+        if (i != j) off += a(i, j) * a(i, j);
+      }
+    if (off <= 1e-32 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; k++) {
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = cs * akp - sn * akq;
+          a(k, q) = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; k++) {
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = cs * apk - sn * aqk;
+          a(q, k) = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; k++) {
+          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = cs * vkp - sn * vkq;
+          V[(size_t)k * n + q] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  std::vector<int> idx(n);
+  for (int i = 0; i < n; i++) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  std::vector<double> Vs((size_t)n * n);
+  vals.resize(n);
+  for (int j = 0; j < n; j++) {
+    vals[j] = a(idx[j], idx[j]);
+    for (int i = 0; i < n; i++) Vs[(size_t)i * n + j] = V[(size_t)i * n + idx[j]];
+  }
+  V = Vs;
+}
+
+// X (k fields) <- orthonormal basis of their span, in order (the Gram-Schmidt
+// loops of LOBPCG.cpp:81-93, 262-267, 443-449), by two Cholesky-QR passes.
+int orthonormalize(spm_ctx *c, void *const *X, int k) {
+  std::vector<double> G, B;
+  for (int pass = 0; pass < 2; pass++) {
+    SPM_TRY(gram(c, X, k, X, k, G));
+    std::vector<int> keep(k, 1);
+    gs_coefficients(G, k, 0.0, keep, B);
+    for (int j = 0; j < k; j++)
+      if (!keep[j]) return spm_fail(SPM_ERR_NONFINITE, "block vectors are linearly dependent");
+    SPM_TRY(combine(c, X, k, X, k, B, nullptr, false));
+  }
+  return SPM_OK;
+}
+
+// X (n fields) <- X - Q (Q^T X), twice (block classical Gram-Schmidt).
+int project_out(spm_ctx *c, void *const *Q, int nq, void *const *X, int n) {
+  std::vector<double> T;
+  for (int pass = 0; pass < 2; pass++) {
+    SPM_TRY(gram(c, Q, nq, X, n, T));
+    for (double &v : T) v = -v;
+    SPM_TRY(combine(c, Q, nq, X, n, T, nullptr, true));
+  }
+  return SPM_OK;
+}
+
+// Orthonormalise X in order with dropping (threshold thr), then once more
+// on the kept vectors; dropped vectors become zero. keep is in/out.
+int orth_with_drop(spm_ctx *c, void *const *X, int k, double thr, std::vector<int> &keep) {
+  std::vector<double> G, B;
+  SPM_TRY(gram(c, X, k, X, k, G));
+  gs_coefficients(G, k, thr, keep, B);
+  SPM_TRY(combine(c, X, k, X, k, B, nullptr, false));
+  SPM_TRY(gram(c, X, k, X, k, G));
+  std::vector<int> keep2 = keep;
+  gs_coefficients(G, k, 0.0, keep2, B);
+  SPM_TRY(combine(c, X, k, X, k, B, nullptr, false));
+  return SPM_OK;
+}
+
+int copy_fields(spm_ctx *c, void *dst, const void *src, int k) {
+  if (dst == src) return SPM_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, src, c->field_bytes * (size_t)k, cudaMemcpyDeviceToDevice, c->stream);
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "field copy");
+}
+
+}  // namespace
+
+void spm_free_extra(spm_ctx *c) {
+  if (!c->extra) return;
+  Solver *s = solver(c);
+  cudaFree(s->gram_part);
+  cudaFree(s->gram_ticket);
+  cudaFree(s->gram_out);
+  cudaFree(s->coef);
+  cudaFree(s->lob);
+  cudaFree(s->spm);
+  cudaFree(s->spm_stats);
+  if (s->h_gram) cudaFreeHost(s->h_gram);
+  delete s;
+  c->extra = nullptr;
+}
+
+// ------------------------------------------------------------------ LOBPCG
+extern "C" int spm_lobpcg_init(spm_ctx *c, void *V, int k, uint64_t seed) {
+  if (!c || !V || k < 1 || k > kBlkMax / 3) return spm_fail(SPM_ERR_ARG, "k must be in [1, 8]");
+  SPM_TRY(ensure_base(c));
+  c->launches++;
+  if (c->prec == SPM_FP64)
+    lobpcg_random_kernel<double><<<1184, 256, 0, c->stream>>>((double *)V, k, npts(c), seed);
+  else
+    lobpcg_random_kernel<float><<<1184, 256, 0, c->stream>>>((float *)V, k, npts(c), seed);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return spm_fail_cuda(e, "random block");
+  std::vector<void *> X(k);
+  for (int i = 0; i < k; i++) X[i] = fld(c, V, i);
+  // each row minus its mean (LOBPCG.cpp:67-79), then Gram-Schmidt (:81-93)
+  std::vector<double> mu;
+  SPM_TRY(means(c, X.data(), k, mu));
+  std::vector<double> I((size_t)k * k, 0.0), d(k);
+  for (int i = 0; i < k; i++) {
+    I[(size_t)i * k + i] = 1.0;
+    d[i] = -mu[i];
+  }
+  SPM_TRY(combine(c, X.data(), k, X.data(), k, I, &d, false));
+  return orthonormalize(c, X.data(), k);
+}
+
+extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
+                          double *resid, int *iters) {
+  if (!c || !phi || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0)
+    return spm_fail(SPM_ERR_ARG, "bad argument (k must be in [1, 8])");
+  SPM_TRY(ensure_base(c));
+  Solver *s = solver(c);
+  if (s->lob_k < k) {
+    cudaFree(s->lob);
+    s->lob = nullptr;
+    s->lob_k = 0;
+    cudaError_t e = cudaMalloc(&s->lob, c->field_bytes * (size_t)(6 * k));
+    if (e != cudaSuccess) return spm_fail_cuda(e, "LOBPCG work fields");
+    s->lob_k = k;
+  }
+  std::vector<void *> Vc(k), U(k), W(k), Y(k), P(k), Up(k), Vn(k);
+  for (int i = 0; i < k; i++) {
+    Vc[i] = fld(c, V, i);
+    U[i] = fld(c, s->lob, i);
+    W[i] = fld(c, s->lob, k + i);
+    Y[i] = fld(c, s->lob, 2 * k + i);
+    P[i] = fld(c, s->lob, 3 * k + i);
+    Up[i] = fld(c, s->lob, 4 * k + i);
+    Vn[i] = fld(c, s->lob, 5 * k + i);
+  }
+  std::vector<double> G, T;
+  std::vector<double> alpha(k, 0.0), res(k, 0.0);
+  SPM_TRY(orthonormalize(c, Vc.data(), k));  // LOBPCG.cpp:262-267
+  int it = 0;
+  bool have_p = false;
+  for (;; it++) {
+    // U = H V, alpha = <V, U>, W = U - alpha V and its norm (the residual)
+    SPM_TRY(hv_many(c, phi, Vc.data(), U.data(), k));
+    SPM_TRY(gram(c, Vc.data(), k, U.data(), k, G));
+    for (int i = 0; i < k; i++) alpha[i] = G[(size_t)i * k + i];
+    {
+      std::vector<void *> X(2 * k);
+      std::vector<double> C((size_t)2 * k * k, 0.0);
+      for (int i = 0; i < k; i++) {
+        X[i] = U[i];
+        X[k + i] = Vc[i];
+        C[(size_t)i * k + i] = 1.0;
+        C[(size_t)(k + i) * k + i] = -alpha[i];
+      }
+      SPM_TRY(combine(c, X.data(), 2 * k, W.data(), k, C, nullptr, false));
+    }
+    SPM_TRY(gram(c, W.data(), k, W.data(), k, G));
+    double rmax = 0.0;
+    for (int i = 0; i < k; i++) {
+      res[i] = std::sqrt(std::max(0.0, G[(size_t)i * k + i]));
+      rmax = std::max(rmax, res[i]);
+    }
+    if (it >= maxiter || (tol > 0 && rmax <= tol)) break;
+    // W = P0(precond(W)), W perp V, W Gram-Schmidt with dropping (LOBPCG.cpp:287-308)
+    SPM_TRY(precond_many(c, W.data(), k));
+    SPM_TRY(project_out(c, Vc.data(), k, W.data(), k));
+    std::vector<int> keepW(k, 1), keepP(k, 0);
+    SPM_TRY(orth_with_drop(c, W.data(), k, 1e-8, keepW));
+    SPM_TRY(hv_many(c, phi, W.data(), Y.data(), k));
+    // P perp [V, W], Gram-Schmidt with dropping, Up = H P (LOBPCG.cpp:311-330)
+    if (have_p) {
+      std::vector<void *> VW(2 * k);
+      for (int i = 0; i < k; i++) {
+        VW[i] = Vc[i];
+        VW[k + i] = W[i];
+      }
+      SPM_TRY(project_out(c, VW.data(), 2 * k, P.data(), k));
+      keepP.assign(k, 1);
+      SPM_TRY(orth_with_drop(c, P.data(), k, 1e-8, keepP));
+      SPM_TRY(hv_many(c, phi, P.data(), Up.data(), k));
+    }
+    // Rayleigh-Ritz on S = [V; W; P] (kept vectors), LOBPCG.cpp:332-403
+    std::vector<void *> S, HS;
+    for (int i = 0; i < k; i++) {
+      S.push_back(Vc[i]);
+      HS.push_back(U[i]);
+    }
+    for (int i = 0; i < k; i++)
+      if (keepW[i]) {
+        S.push_back(W[i]);
+        HS.push_back(Y[i]);
+      }
+    for (int i = 0; i < k; i++)
+      if (keepP[i]) {
+        S.push_back(P[i]);
+        HS.push_back(Up[i]);
+      }
+    const int m = (int)S.size();
+    SPM_TRY(gram(c, S.data(), m, HS.data(), m, G));
+    std::vector<double> Gs((size_t)m * m), vals, vecs;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < m; j++) Gs[(size_t)i * m + j] = (G[(size_t)j * m + i] + G[(size_t)i * m + j]) * 0.5;
+    sym_eig(Gs, m, vals, vecs);
+    // V_new = eta_k^T S; P <- V_old (LOBPCG.cpp:391-419)
+    std::vector<double> C((size_t)m * k);
+    for (int p = 0; p < m; p++)
+      for (int q = 0; q < k; q++) C[(size_t)p * k + q] = vecs[(size_t)p * m + q];
+    SPM_TRY(combine(c, S.data(), m, Vn.data(), k, C, nullptr, false));
+    std::swap(P, Vc);   // P holds the old V
+    std::swap(Vc, Vn);  // V holds the new block
+    have_p = true;
+    // mean removal and Gram-Schmidt of the new block (LOBPCG.cpp:428-449)
+    std::vector<double> mu;
+    SPM_TRY(means(c, Vc.data(), k, mu));
+    std::vector<double> I((size_t)k * k, 0.0), d(k);
+    for (int i = 0; i < k; i++) {
+      I[(size_t)i * k + i] = 1.0;
+      d[i] = -mu[i];
+    }
+    SPM_TRY(combine(c, Vc.data(), k, Vc.data(), k, I, &d, false));
+    SPM_TRY(orthonormalize(c, Vc.data(), k));
+  }
+  // the caller's buffer receives the final block
+  for (int i = 0; i < k; i++) SPM_TRY(copy_fields(c, fld(c, V, i), Vc[i], 1));
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "lobpcg");
+  if (evals) std::copy(alpha.begin(), alpha.end(), evals);
+  if (resid) std::copy(res.begin(), res.end(), resid);
+  if (iters) *iters = it;
+  return SPM_OK;
+}
+
+// ------------------------------------------------------------------ SPM
+static int ensure_spm(spm_ctx *c, int cap) {
+  SPM_TRY(ensure_base(c));
+  Solver *s = solver(c);
+  if (!s->spm) {
+    cudaError_t e = cudaMalloc(&s->spm, c->field_bytes * 3);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "SPM work fields");
+  }
+  if (s->spm_cap < cap) {
+    cudaFree(s->spm_stats);
+    s->spm_stats = nullptr;
+    s->spm_cap = 0;
+    cudaError_t e = cudaMalloc(&s->spm_stats, sizeof(double) * (size_t)std::max(cap, 1024));
+    if (e != cudaSuccess) return spm_fail_cuda(e, "SPM stats");
+    s->spm_cap = std::max(cap, 1024);
+  }
+  return spm_ensure_scratch(c, 2);
+}
+
+extern "C" int spm_get_tv(spm_ctx *c, const void *phi0, const void *phi1, void *v) {
+  if (!c || !phi0 || !phi1 || !v) return spm_fail(SPM_ERR_ARG, "null argument");
+  SPM_TRY(ensure_spm(c, 0));
+  Solver *s = solver(c);
+  return spm_table_of(c)->tangent(c, phi0, phi1, v, fld(c, s->spm, 1), fld(c, s->spm, 2));
+}
+
+static int force_step(spm_ctx *c, void *x, const void *v, double factor) {
+  if (!c || !x || !v) return spm_fail(SPM_ERR_ARG, "null argument");
+  SPM_TRY(ensure_spm(c, 0));
+  Solver *s = solver(c);
+  const OpsTable *t = spm_table_of(c);
+  SPM_TRY(t->tangent(c, nullptr, v, nullptr, fld(c, s->spm, 1), fld(c, s->spm, 2)));
+  void *xs[1] = {x};
+  return t->force(c, xs, 1, v, fld(c, s->spm, 1), fld(c, s->spm, 2), factor);
+}
+
+extern "C" int spm_natural_forces(spm_ctx *c, void *x, const void *v) { return force_step(c, x, v, 1.0); }
+extern "C" int spm_minmax_forces(spm_ctx *c, void *x, const void *v) { return force_step(c, x, v, 2.0); }
+
+static __global__ void spm_flow_init_kernel(int *flow) {
+  flow[FW_GO] = 1;
+  flow[FW_PENDING] = 0;
+  flow[FW_ITER] = 0;
+}
+
+// One Spring_Pairing iteration (SPM.cpp:191-255), gated by c->gate.
+static int spm_iteration(spm_ctx *c, void *phi0, void *phi1, double tol, int cap) {
+  Solver *s = solver(c);
+  const OpsTable *t = spm_table_of(c);
+  void *v = fld(c, s->spm, 0), *vh = fld(c, s->spm, 1), *gv = fld(c, s->spm, 2);
+  void *X[2] = {phi0, phi1};
+  const size_t n = npts(c);
+  const double dt = 0.001, ks = 1.0;  // SPM.cpp:177-178
+  SPM_TRY(t->tangent(c, phi0, phi1, v, vh, gv));
+  SPM_TRY(t->force(c, X, 2, v, vh, gv, 1.0));
+  c->launches++;
+  if (c->prec == SPM_FP64)
+    spring_kernel<double><<<1184, 256, 0, c->stream>>>((double *)phi0, (double *)phi1, n, dt, ks, c->gate);
+  else
+    spring_kernel<float><<<1184, 256, 0, c->stream>>>((float *)phi0, (float *)phi1, n, dt, ks, c->gate);
+  SPM_TRY(t->tangent(c, phi0, phi1, v, vh, gv));
+  SPM_TRY(t->force(c, X, 2, v, vh, gv, 2.0));
+  SPM_TRY(t->gnorm(c, (const void *const *)X, 2));
+  c->launches += 2;
+  if (c->prec == SPM_FP64)
+    spring_kernel<double><<<1184, 256, 0, c->stream>>>((double *)phi0, (double *)phi1, n, dt, ks, c->gate);
+  else
+    spring_kernel<float><<<1184, 256, 0, c->stream>>>((float *)phi0, (float *)phi1, n, dt, ks, c->gate);
+  spm_check_kernel<<<1, 1, 0, c->stream>>>(c->scal, c->gate, s->spm_stats, tol, cap);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "spm iteration");
+}
+
+extern "C" int spm_spring_pairing(spm_ctx *c, void *phi0, void *phi1, int maxiter, double tol, double *res_hist,
+                                  int *iters) {
+  if (!c || !phi0 || !phi1 || maxiter < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (iters) *iters = 0;
+  if (maxiter == 0) return SPM_OK;
+  SPM_TRY(ensure_spm(c, maxiter));
+  Solver *s = solver(c);
+  c->launches++;
+  spm_flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
+  c->gate = c->flow;
+  int enq = 0, chunk = 4, rc = SPM_OK;
+  cudaError_t e = cudaSuccess;
+  while (enq < maxiter && rc == SPM_OK) {
+    const int n = std::min(chunk, maxiter - enq);
+    for (int i = 0; i < n && rc == SPM_OK; i++) rc = spm_iteration(c, phi0, phi1, tol, s->spm_cap);
+    if (rc != SPM_OK) break;
+    enq += n;
+    e = cudaMemcpyAsync(c->host_flow, c->flow, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      rc = spm_fail_cuda(e, "spring pairing");
+      break;
+    }
+    if (c->host_flow[FW_GO] == 0) break;
+    chunk = std::min(chunk * 2, 64);
+  }
+  c->gate = nullptr;
+  if (rc != SPM_OK) return rc;
+  const int done = c->host_flow[FW_ITER];
+  if (iters) *iters = done;
+  if (res_hist && done > 0) {
+    e = cudaMemcpy(res_hist, s->spm_stats, sizeof(double) * (size_t)done, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "spm stats");
+    for (int i = 0; i < done; i++)
+      if (!std::isfinite(res_hist[i])) return spm_fail(SPM_ERR_NONFINITE, "non-finite SPM residual");
+  }
+  return SPM_OK;
+}

@@ -50,7 +50,7 @@ extern "C" int spm_supported_size(int N) {
 }
 
 // ------------------------------------------------------------------ dispatch
-static const OpsTable *table_of(const spm_ctx *c) {
+const OpsTable *spm_table_of(const spm_ctx *c) {
   switch (c->N) {
     case 32: return spm_table_32(c->prec);
     case 64: return spm_table_64(c->prec);
@@ -78,6 +78,7 @@ KParams spm_params(const spm_ctx *c) {
   p.partials = c->partials;
   p.tickets = c->tickets;
   p.scal = c->scal;
+  p.flow = c->gate;
   return p;
 }
 
@@ -216,13 +217,13 @@ extern "C" uint64_t spm_launch_count(const spm_ctx *c) { return c ? c->launches 
 extern "C" int spm_fft(spm_ctx *c, const void *x, void *xhat) {
   if (!c || !x || !xhat) return spm_fail(SPM_ERR_ARG, "null argument");
   SPM_TRY(spm_ensure_scratch(c, 1));
-  return table_of(c)->fft(c, x, xhat);
+  return spm_table_of(c)->fft(c, x, xhat);
 }
 
 extern "C" int spm_ifft(spm_ctx *c, const void *xhat, void *x) {
   if (!c || !x || !xhat) return spm_fail(SPM_ERR_ARG, "null argument");
   SPM_TRY(spm_ensure_scratch(c, 1));
-  return table_of(c)->ifft(c, xhat, x);
+  return spm_table_of(c)->ifft(c, xhat, x);
 }
 
 extern "C" int spm_spectrum_to_full(spm_ctx *c, const void *xhat, double *full) {
@@ -250,7 +251,7 @@ extern "C" int spm_spectrum_from_full(spm_ctx *c, const double *full, void *xhat
 // ------------------------------------------------------------------ energy, gradient
 extern "C" int spm_energy(spm_ctx *c, const void *phi, const void *uhat, double *energy) {
   if (!c || !phi || !uhat || !energy) return spm_fail(SPM_ERR_ARG, "null argument");
-  SPM_TRY(table_of(c)->energy(c, phi, uhat));
+  SPM_TRY(spm_table_of(c)->energy(c, phi, uhat));
   SPM_TRY(spm_read_scal(c, 1));
   *energy = c->host_scal[SC_E1] + c->host_scal[SC_E2];
   if (!std::isfinite(*energy)) return spm_fail(SPM_ERR_NONFINITE, "energy is not finite");
@@ -283,7 +284,7 @@ extern "C" int spm_grad_flow_enqueue(spm_ctx *c, void *phi, void *uhat, int nste
   SPM_TRY(ensure_stats(c, nsteps));
   c->launches++;
   flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
-  const OpsTable *t = table_of(c);
+  const OpsTable *t = spm_table_of(c);
   c->m.tol_grad = tol_grad;
   int rc = SPM_OK;
   for (int i = 0; i < nsteps && rc == SPM_OK; i++) rc = t->grad_step(c, phi, uhat);
@@ -318,7 +319,7 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
   SPM_TRY(ensure_stats(c, max_steps));
   c->launches++;
   flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
-  const OpsTable *t = table_of(c);
+  const OpsTable *t = spm_table_of(c);
   c->m.tol_grad = tol_grad;
   int enq = 0, chunk = 8, rc = SPM_OK;
   cudaError_t e = cudaSuccess;
@@ -365,7 +366,7 @@ extern "C" int spm_grad_step_profile(spm_ctx *c, void *phi, void *uhat, int reps
   for (int i = 0; i < 4; i++) cudaEventCreate(&ev[i]);
   double acc[3] = {0, 0, 0};
   int rc = SPM_OK;
-  const OpsTable *t = table_of(c);
+  const OpsTable *t = spm_table_of(c);
   for (int r = 0; r < reps && rc == SPM_OK; r++) {
     rc = t->grad_step_ev(c, phi, uhat, (void *const *)ev);
     if (rc != SPM_OK) break;
@@ -385,7 +386,7 @@ extern "C" int spm_grad_step_profile(spm_ctx *c, void *phi, void *uhat, int reps
 extern "C" int spm_ngrad(spm_ctx *c, const void *phi, void *grad, double *norm) {
   if (!c || !phi || !grad) return spm_fail(SPM_ERR_ARG, "null argument");
   SPM_TRY(spm_ensure_scratch(c, 1));
-  SPM_TRY(table_of(c)->ngrad(c, phi, grad));
+  SPM_TRY(spm_table_of(c)->ngrad(c, phi, grad));
   if (norm) {
     SPM_TRY(spm_read_scal(c, 1));
     *norm = std::sqrt(c->host_scal[SC_GN2]);
@@ -405,7 +406,7 @@ extern "C" int spm_hv(spm_ctx *c, const void *phi, const void *v, void *hv, int 
       vv[b] = (const char *)v + c->field_bytes * (size_t)(b0 + b);
       hh[b] = (char *)hv + c->field_bytes * (size_t)(b0 + b);
     }
-    SPM_TRY(table_of(c)->hv(c, phi, vv, hh, n));
+    SPM_TRY(spm_table_of(c)->hv(c, phi, vv, hh, n));
   }
   return SPM_OK;
 }
@@ -417,14 +418,14 @@ extern "C" int spm_precond(spm_ctx *c, void *w, int nb) {
     SPM_TRY(spm_ensure_scratch(c, n));
     void *ww[kMaxBatch];
     for (int b = 0; b < n; b++) ww[b] = (char *)w + c->field_bytes * (size_t)(b0 + b);
-    SPM_TRY(table_of(c)->precond(c, ww, n));
+    SPM_TRY(spm_table_of(c)->precond(c, ww, n));
   }
   return SPM_OK;
 }
 
 extern "C" int spm_inpfp(spm_ctx *c, const void *pp, const void *qq, double *out) {
   if (!c || !pp || !qq || !out) return spm_fail(SPM_ERR_ARG, "null argument");
-  SPM_TRY(table_of(c)->dot(c, pp, qq));
+  SPM_TRY(spm_table_of(c)->dot(c, pp, qq));
   SPM_TRY(spm_read_scal(c, 1));
   *out = c->host_scal[SC_SUM0];
   return SPM_OK;

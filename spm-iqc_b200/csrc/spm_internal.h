@@ -30,6 +30,7 @@ struct spm_ctx {
   void *extra = nullptr;        // solver state (LOBPCG / SPM work arrays)
   void *host_phi = nullptr;     // device copies used by the host-buffer entry points
   void *host_uhat = nullptr;
+  int *gate = nullptr;          // flow words gating every launch of a solver chain (or null)
 };
 
 int spm_fail(int status, const char *what);
@@ -40,3 +41,4 @@ char *spm_bufA(spm_ctx *c, int b);
 char *spm_bufB(spm_ctx *c, int b);
 int spm_read_scal(spm_ctx *c, int nb);
 void spm_free_extra(spm_ctx *c);
+const struct OpsTable *spm_table_of(const spm_ctx *c);

@@ -15,6 +15,9 @@ struct OpsTable {
   int (*hv)(spm_ctx *, const void *phi, const void *const *v, void *const *hv, int n);
   int (*precond)(spm_ctx *, void *const *w, int n);
   int (*dot)(spm_ctx *, const void *p, const void *q);
+  int (*tangent)(spm_ctx *, const void *phi0, const void *phi1, void *v_out, void *vhat, void *gv);
+  int (*force)(spm_ctx *, void *const *x, int n, const void *v, const void *vhat, const void *gv, double factor);
+  int (*gnorm)(spm_ctx *, const void *const *x, int n);
 };
 
 // prec: 0 = FP64, 1 = FP32

@@ -60,6 +60,15 @@ def lib():
             "spm_precond": [_vp, _vp, ctypes.c_int],
             "spm_inpfp": [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
             "spm_supported_size": [ctypes.c_int],
+            "spm_lobpcg_init": [_vp, _vp, ctypes.c_int, ctypes.c_uint64],
+            "spm_lobpcg": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_int)],
+            "spm_get_tv": [_vp, _vp, _vp, _vp],
+            "spm_natural_forces": [_vp, _vp, _vp],
+            "spm_minmax_forces": [_vp, _vp, _vp],
+            "spm_spring_pairing": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -186,6 +195,45 @@ class SpmContext:
         nb = 1 if w.dim() == 3 else w.shape[0]
         check(lib().spm_precond(self.h, _ptr(w), nb))
         return w
+
+    def hiosd_lobpcg_initialization(self, k: int, seed: int = 0):
+        """Random mean-free orthonormal start block, shape (k, N, N, N)."""
+        V = self.field(k)
+        check(lib().spm_lobpcg_init(self.h, _ptr(V), int(k), ctypes.c_uint64(seed)))
+        return V
+
+    def hiosd_lobpcg_inip(self, phi, V, maxiter: int = 21, tol: float = 0.0):
+        """maxiter LOBPCG iterations on V (k, N, N, N) in place; returns
+        (evals, residuals, iterations)."""
+        k = V.shape[0]
+        ev = (ctypes.c_double * k)()
+        rs = (ctypes.c_double * k)()
+        it = ctypes.c_int()
+        check(lib().spm_lobpcg(self.h, _ptr(phi), _ptr(V), int(k), int(maxiter), float(tol), ev, rs,
+                               ctypes.byref(it)))
+        return np.array(ev[:]), np.array(rs[:]), it.value
+
+    # ---- SPM.cpp
+    def get_Tv(self, phi0, phi1, v=None):
+        v = self.field() if v is None else v
+        check(lib().spm_get_tv(self.h, _ptr(phi0), _ptr(phi1), _ptr(v)))
+        return v
+
+    def Natural_Forces(self, x, v):
+        check(lib().spm_natural_forces(self.h, _ptr(x), _ptr(v)))
+        return x
+
+    def MinMax_Forces(self, x, v):
+        check(lib().spm_minmax_forces(self.h, _ptr(x), _ptr(v)))
+        return x
+
+    def Spring_Pairing(self, phi0, phi1, maxiter: int, tol: float):
+        """Runs the spring pair iteration in place; returns the residual history."""
+        hist = (ctypes.c_double * max(1, maxiter))()
+        it = ctypes.c_int()
+        check(lib().spm_spring_pairing(self.h, _ptr(phi0), _ptr(phi1), int(maxiter), float(tol), hist,
+                                       ctypes.byref(it)))
+        return np.array(hist[:it.value])
 
     # ---- BasicOperators.cpp
     def inpfp(self, p, q) -> float:

@@ -1,0 +1,121 @@
+"""CUDA LOBPCG and Spring Pair Method vs the FP64 oracle (1e-11 relative for
+fields and eigenvalues; eigenvectors compared as subspaces)."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from oracle import spmiqc_np as npo
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-11
+
+
+@pytest.fixture(scope="module")
+def spm(cuda):
+    import spmiqc
+    return spmiqc
+
+
+def t(cuda, a):
+    return cuda.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def subspace_ritz(m, phi, V):
+    """Eigenvalues of V^T H V / N^3 for an orthonormal block (rotation invariant)."""
+    k = V.shape[0]
+    HV = np.stack([m.hv(phi, V[i]) for i in range(k)])
+    M = np.array([[m.inpfp(V[i], HV[j]) for j in range(k)] for i in range(k)])
+    return np.linalg.eigvalsh(0.5 * (M + M.T))
+
+
+@pytest.mark.parametrize("N,k", [(32, 3), (64, 2)])
+def test_lobpcg_init_matches_oracle(spm, cuda, N, k):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    V = ctx.hiosd_lobpcg_initialization(k, seed=5).cpu().numpy()
+    ref = m.lobpcg_init(k, 5)
+    assert rel(V, ref) < TOL
+
+
+@pytest.mark.parametrize("N,k,iters", [(32, 3, 6), (64, 4, 8)])
+def test_lobpcg_matches_oracle(spm, cuda, N, k, iters):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 7)
+    V0 = m.lobpcg_init(k, 5)
+    Vd = t(cuda, V0)
+    ev, rs, it = ctx.hiosd_lobpcg_inip(t(cuda, phi), Vd, iters)
+    assert it == iters
+    Vg = Vd.cpu().numpy()
+    Vr, _ = m.lobpcg_inip(phi, V0, iters)
+    # eigenvalues of the block (rotation invariant) and per-vector Rayleigh quotients
+    rg, rr = subspace_ritz(m, phi, Vg), subspace_ritz(m, phi, Vr)
+    assert np.max(np.abs(rg - rr)) <= TOL * np.max(np.abs(rr))
+    assert np.max(np.abs(np.sort(ev) - rr)) <= 1e-9 * np.max(np.abs(rr))
+    # the two blocks span the same subspace (principal angles)
+    s = np.linalg.svd(Vg.reshape(k, -1) @ Vr.reshape(k, -1).T / N ** 3, compute_uv=False)
+    assert np.min(s) > 1 - 1e-9
+    # orthonormal and mean free
+    G = Vg.reshape(k, -1) @ Vg.reshape(k, -1).T / N ** 3
+    assert np.max(np.abs(G - np.eye(k))) < 1e-12
+    assert np.max(np.abs(Vg.reshape(k, -1).mean(1))) < 1e-14
+
+
+def test_lobpcg_at_zero_field_finds_lowest_kernel_modes(spm, cuda):
+    """Known answer: H(0) is diagonal in k with eigenvalues G(k) - Tau. With
+    L = 5 on a 32^3 grid the |n| = 5 shell (30 modes, k^2 = 1, G = min) is an
+    exactly degenerate lowest cluster with a clear gap above it."""
+    N, L = 32, 5.0
+    m = npo.Model(N, L=L)
+    ctx = spm.SpmContext(N, L=L)
+    phi = cuda.zeros((N,) * 3, dtype=cuda.float64, device="cuda")
+    V = ctx.hiosd_lobpcg_initialization(2, seed=1)
+    ev, rs, it = ctx.hiosd_lobpcg_inip(phi, V, 100, tol=1e-8)
+    k2 = m.k2.ravel()  # the k = 0 mode is excluded: the block is kept mean free
+    exact = np.sort((m.G - m.Tau).ravel()[k2 > 0])[:2]
+    assert it < 100 and np.max(rs) <= 1e-8
+    # eigenvalue error ~ residual^2 / gap ~ 1e-13 absolute
+    assert np.allclose(np.sort(ev), exact, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("N", [32, 64])
+def test_tangent_and_force_steps(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 3)
+    d = npo.uniform_field(N, 4, amp=1.0)
+    v = ctx.get_Tv(t(cuda, phi), t(cuda, phi + 0.01 * d)).cpu().numpy()
+    vr = m.tangent(phi, phi + 0.01 * d)
+    assert rel(v, vr) < TOL
+    x = t(cuda, phi)
+    ctx.Natural_Forces(x, t(cuda, vr))
+    assert rel(x.cpu().numpy(), m.natural_forces(phi, vr)) < TOL
+    x = t(cuda, phi)
+    ctx.MinMax_Forces(x, t(cuda, vr))
+    assert rel(x.cpu().numpy(), m.minmax_forces(phi, vr)) < TOL
+
+
+@pytest.mark.parametrize("N", [32, 64])
+def test_spring_pairing(spm, cuda, N):
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 9)
+    d = npo.uniform_field(N, 10, amp=1.0)
+    vr = m.tangent(phi, phi + d)
+    p0, p1 = t(cuda, phi), t(cuda, phi + 0.001 * vr)
+    hist = ctx.Spring_Pairing(p0, p1, 4, 1e-9)
+    a, b, it, res = m.spring_pairing(phi, phi + 0.001 * vr, 4, 1e-9)
+    assert len(hist) == it == 4
+    assert abs(hist[-1] - res) <= 1e-9 * res
+    assert rel(p0.cpu().numpy(), a) < TOL and rel(p1.cpu().numpy(), b) < TOL
+
+
+def test_spring_pairing_stops_at_tolerance(spm, cuda):
+    N = 32
+    m = npo.Model(N)
+    ctx = spm.SpmContext(N)
+    phi = npo.uniform_field(N, 9)
+    vr = m.tangent(phi, phi + npo.uniform_field(N, 10, amp=1.0))
+    p0, p1 = t(cuda, phi), t(cuda, phi + 0.001 * vr)
+    hist = ctx.Spring_Pairing(p0, p1, 50, 1e3)  # the first residual is below the tolerance
+    assert len(hist) == 1
