@@ -77,6 +77,12 @@ int spm_supported_size(int N);
 size_t spm_field_bytes(const spm_ctx *ctx);
 size_t spm_spectrum_bytes(const spm_ctx *ctx);
 const char *spm_status_str(int status);
+/* Tuning knobs (no counterpart in the reference; the analogue of FFTW's plan
+ * choice, My_FFT.cpp:49-97). knob "plane_cps": 1 = plane kernels stage their
+ * input in shared memory (one CTA per SM), 2 = direct loads, two CTAs per SM.
+ * spm_tune_get returns the current value or -1 for an unknown knob. */
+int spm_tune(spm_ctx *ctx, const char *knob, int value);
+int spm_tune_get(const spm_ctx *ctx, const char *knob);
 const char *spm_last_error(void);
 /* Number of transform-kernel launches issued by this context so far. */
 uint64_t spm_launch_count(const spm_ctx *ctx);

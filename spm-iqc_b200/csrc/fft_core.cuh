@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cooperative_groups.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -256,6 +257,66 @@ __device__ __forceinline__ bool grid_reduce(double (&acc)[NR], double *scratch, 
   return false;
 }
 
+// ------------------------------------------------------------------ async copies
+// Bulk global->shared copies completing on an mbarrier (the non-tensor TMA
+// path), and bounded waits: a wait that does not complete within ~1 s sets
+// the CTA's error word and reports failure instead of spinning forever.
+__device__ __forceinline__ uint32_t smem_u32(const void *ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// dst/src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Tiled 3D tensor copy global->shared (coordinates innermost first, in
+// elements; the innermost coordinate times the element size is a multiple of
+// 16 bytes at every call site).
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+constexpr long kSpinLimit = 4L << 20;  // polls of ~256 ns: about 1 s
+// Returns false (and sets *err) when the phase did not complete in time.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+  if (*((volatile int *)err)) return false;
+  for (long i = 0; i < kSpinLimit; i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (i > 16) __nanosleep(256);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
 // ------------------------------------------------------------------ parameters
 struct ModelC {
   double Tau, Gamma, dt;
@@ -269,9 +330,13 @@ struct ModelC {
 };
 
 // Grad-flow control words in device memory.
-enum FlowWord { FW_GO = 0, FW_PENDING = 1, FW_ITER = 2 };
+enum FlowWord { FW_GO = 0, FW_PENDING = 1, FW_ITER = 2, FW_ERR = 4 };
 
 struct KParams {
+  // Tensor maps of the strided inputs: tmi[b] over p.in[b], tms[b] over p.st[b]
+  // (filled by the launcher for the kernels that stage through TMA).
+  CUtensorMap tmi[kMaxBatch];
+  CUtensorMap tms[kMaxBatch];
   ModelC m;
   const void *in[kMaxBatch];
   void *out[kMaxBatch];
@@ -285,26 +350,19 @@ struct KParams {
   double *scal;         // [nb][kScal]
   int *flow;            // grad-flow control words (or null)
   double *stats;        // grad-flow per-step records (or null)
+  const double4 *gtab;  // per K^2 = Kx^2+Ky^2+Kz^2: {G, 1/(1+dt G), 1/(G+|Tau|+0.02), 1/(1+G)}
+  int *err;             // set when a bounded wait timed out
   int nb;
 };
 
+// Spectral symbols of wave vector (Kx, Ky, Kz) from the per-context table.
+__device__ __forceinline__ double4 symbols(const KParams &p, int Kx, int Ky, int Kz) {
+  const double2 *t = reinterpret_cast<const double2 *>(p.gtab) + 2 * (Kx * Kx + Ky * Ky + Kz * Kz);
+  const double2 a = __ldg(t), c = __ldg(t + 1);
+  return make_double4(a.x, a.y, c.x, c.y);
+}
+
 // Signed wave number of index i on an N grid (Initialization.cpp:97-107).
 __device__ __forceinline__ int wave(int i, int N) { return i < N / 2 ? i : i - N; }
-
-// Pair kernel G at integer wave vector (Kx, Ky, Kz): k^2 = ((px^2 + py^2) + pz^2),
-// p = K / L as the reference builds it (Initialization.cpp:132-148), then
-// get_GK (Initialization.cpp:150-166). Rounded multiplies/adds keep the k^2
-// arithmetic identical to the reference's; exp is CUDA's.
-__device__ __forceinline__ double gk_of(int Kx, int Ky, int Kz, double invL) {
-  double px = __dmul_rn(invL, (double)Kx), py = __dmul_rn(invL, (double)Ky),
-         pz = __dmul_rn(invL, (double)Kz);
-  double k2 = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz));
-  const double ph = 0.568809;
-  const double s2 = ph * ph;
-  double k4 = k2 * k2, k6 = k4 * k2, k8 = k6 * k2;
-  double poly = 1.969182919080340 + -14.949858723012090 * k2 + 37.445683882581790 * k4 +
-                -38.839451762550148 * k6 + 13.999261011773505 * k8;
-  return exp(-0.5 * k2 / s2) * poly + 0.08;
-}
 
 }  // namespace spm

@@ -1,24 +1,25 @@
 // The three streaming passes of a fused pseudo-spectral step on an N^3 grid.
 //
-//   plane_fwd : one thread-block cluster per x-plane (CL = N/32 CTAs). Each CTA
-//               loads 32 z-rows of the real field, applies a pointwise prologue
-//               (the nonlinear term, an energy density, ...), does the R2C
-//               z-transform of its rows, then the cluster exchanges columns
-//               through distributed shared memory and each CTA does the
-//               y-transform of 16 spectral columns and writes them out.
-//   pencil    : x-transform of 16 x-pencils (two ky rows {ky, -ky} x 8 columns),
-//               a per-spectral-point operator (gradient step, G multiply,
-//               preconditioner, SPM force update, ...) with reductions, and the
-//               inverse x-transform, all without leaving the SM.
-//   plane_inv : inverse of plane_fwd (y then C2R z) with a pointwise epilogue.
+//   plane_fwd : thread-block clusters of CL = N/32 CTAs, each cluster looping
+//               over x-planes. Each CTA takes 32 z-rows of the real field,
+//               applies a pointwise prologue (the nonlinear term, an energy
+//               density, ...), does the R2C z-transform of its rows; the
+//               cluster then exchanges columns through distributed shared
+//               memory and each CTA does the y-transform of 16 spectral columns.
+//   pencil    : CTAs looping over tiles of 16 x-pencils (two ky rows
+//               {ky, -ky} x 8 columns): forward x-transform, a per-spectral-point
+//               operator (gradient step, G multiply, preconditioner, SPM force
+//               update, ...) with reductions, inverse x-transform.
+//   plane_inv : inverse of plane_fwd (y, then C2R z) with a pointwise epilogue.
 //
-// Line transforms are two-level: each thread holds R1 elements of a line in
-// registers (radix-R1 DFT), one shared-memory exchange, then an R2 = 8 or 16
-// point DFT. Twiddles come from a per-grid table in shared memory.
+// All three kernels are persistent: the input of the next tile is fetched
+// with bulk asynchronous copies into a shared-memory stage (completion on an
+// mbarrier) while the current tile is transformed. Line transforms are
+// two-level: each thread holds R1 elements of a line in registers (radix-R1
+// DFT), one shared-memory exchange, then an 8- or 16-point DFT.
 //
-// Every kernel first checks the optional grad-flow "go" word so that a chain of
-// steps enqueued ahead (or replayed from a CUDA graph) stops exactly where the
-// reference's loop would (LPsrc.cpp:52).
+// Every kernel first checks the optional "go" word so that a chain of steps
+// enqueued ahead stops exactly where the reference's loop would (LPsrc.cpp:52).
 #pragma once
 
 #include "fft_core.cuh"
@@ -34,20 +35,31 @@ template <int N> struct Geo {
   static constexpr int ZPAD = N1 + 1;       // padded k1 extent of the z exchange
   static constexpr int PLANE_UNITS = kRows * 8 * ZPAD > kRows * M ? kRows * 8 * ZPAD : kRows * M;
   static constexpr int PENCIL_UNITS = M1 * 16 * 16;   // = 16 N
-  static constexpr int BLOCKS = N * CL;     // CTAs per field, plane kernels (= N^2/32)
-  static constexpr int PBLOCKS = (N / 2) * (M / 8);   // CTAs per field, pencil kernel
-  static_assert(BLOCKS <= kPartStride && PBLOCKS <= kPartStride, "partials stride");
+  static constexpr int STAGE_UNITS = 16 * N;          // one staged tile (plane rows / columns / pencils)
+  static constexpr int PTILES = (N / 2) * (M / 8);    // pencil tiles per field
 };
 
-template <int N, class T> constexpr size_t plane_smem() {
-  return sizeof(c2<T>) * (N + Geo<N>::PLANE_UNITS) + sizeof(double) * 32 * kRedMax;
+// Shared-memory layout (complex units): twiddles N | z-twiddles N/2 | work | stage | mbarriers | reduction
+// (+128 bytes to align the base for the tensor copies)
+template <int N, class T, int CPS> constexpr size_t plane_smem() {
+  return sizeof(c2<T>) * (N + N / 2 + Geo<N>::PLANE_UNITS + (CPS == 1 ? Geo<N>::STAGE_UNITS : 0)) + 16 +
+         sizeof(double) * 32 * kRedMax + 128;
 }
-template <int N, class T> constexpr size_t pencil_smem() {
-  return sizeof(c2<T>) * (N + Geo<N>::PENCIL_UNITS) + sizeof(double) * 32 * kRedMax;
+template <int N, class T> constexpr size_t pencil_smem(int stages) {
+  return sizeof(c2<T>) * (N + Geo<N>::PENCIL_UNITS + (size_t)stages * Geo<N>::STAGE_UNITS) + 16 +
+         sizeof(double) * 32 * kRedMax + 128;
+}
+
+__device__ __forceinline__ unsigned char *smem_base128(unsigned char *raw) {
+  return raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
 }
 
 __device__ __forceinline__ bool flow_stopped(const KParams &p) {
   return p.flow != nullptr && *((volatile const int *)p.flow + FW_GO) == 0;
+}
+
+__device__ __forceinline__ void report_error(const KParams &p, int s_err) {
+  if (s_err && p.err && threadIdx.x == 0) atomicExch(p.err, 1);
 }
 
 // --------------------------------------------------------------- plane_fwd
@@ -55,138 +67,170 @@ __device__ __forceinline__ bool flow_stopped(const KParams &p) {
 //      __device__ static T2 pro(const KParams&, int b, size_t idx, T2 x, double (&acc)[NR]);
 //        (x = reals idx, idx+1 of the input field; returns the values to transform)
 //      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
-template <int N, class T, class Pro>
-__global__ void __launch_bounds__(kThreads) plane_fwd_kernel(const __grid_constant__ KParams p) {
+// CPS = CTAs per SM the variant is built for: 1 stages the next plane's rows
+// in shared memory with a bulk copy; 2 has no stage (half the shared memory,
+// so two CTAs share an SM) and loads its rows straight from global memory.
+template <int N, class T, class Pro, int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
   constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + N;
-  double *red = reinterpret_cast<double *>(buf + G::PLANE_UNITS);
+  constexpr bool STAGED = (CPS == 1);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
+  T2 *ztw = tw + N;                  // ztw[k1*8 + j2] = w^{2 j2 k1}
+  T2 *buf = ztw + N / 2;
+  T2 *stage = buf + G::PLANE_UNITS;  // 32 rows of N reals
+  uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
+  double *red = reinterpret_cast<double *>(bar + 2);
+  __shared__ int s_err;
   if (flow_stopped(p)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
-  const int plane = blockIdx.x / G::CL;
+  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  const T *src = reinterpret_cast<const T *>(p.in[b]);
+  auto issue = [&](int plane) {  // warp 0: one bulk copy per row of this CTA
+    if (lane == 0) mbar_expect_tx(bar, (unsigned)(kRows * N * sizeof(T)));
+    __syncwarp();
+    bulk_g2s(stage + lane * (N / 2), src + ((size_t)plane * N + rank * kRows + lane) * N, N * sizeof(T), bar);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    s_err = 0;
+    fence_barrier_init();
+  }
   for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
+  __syncthreads();
+  for (int i = tid; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
   double acc[Pro::NR > 0 ? Pro::NR : 1];
 #pragma unroll
   for (int r = 0; r < (Pro::NR > 0 ? Pro::NR : 1); r++) acc[r] = ((Pro::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  int plane = cid;
+  if (STAGED && warp == 0 && plane < N) issue(plane);
   __syncthreads();
 
-  // ---- z, stage 1: task (row r, j2), 8 threads per row; element j = j1*8 + j2
-  {
-    const int j2 = tid & 7, r = tid >> 3;
-    const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
-    const T *src = reinterpret_cast<const T *>(p.in[b]) + rowoff;
-    T2 v[N1];
-    sfor<0, N1>([&](auto J1) {
-      constexpr int j1 = SPM_CI(J1);
-      const int j = j1 * 8 + j2;
-      T2 x = __ldg(reinterpret_cast<const T2 *>(src) + j);
-      v[j1] = Pro::pro(p, b, rowoff + 2 * j, x, acc);
-    });
-    Dft<-1, N1, T2>::run(v);
-    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
-    sfor<0, N1>([&](auto K1) {
-      constexpr int k1 = SPM_CI(K1);
-      E[k1] = (k1 == 0) ? v[k1] : cmul(v[k1], tw[2 * j2 * k1]);
-    });
-  }
-  __syncthreads();
-  // ---- z, stage 2: task (r, k1), 8-point DFT over j2 -> k = k1 + N1*k2
-  {
-    constexpr int NT = kRows * N1;
-    constexpr int TPT = (NT + kThreads - 1) / kThreads;
-    T2 u[TPT][8];
+  for (int it = 0; plane < N; plane += ncl, it++) {
+    const int next = plane + ncl;
+    if (STAGED) mbar_wait(bar, it & 1, &s_err);
+    // ---- z, stage 1: task (row r, j2), 8 threads per row; element j = j1*8 + j2
+    {
+      const int j2 = tid & 7, r = tid >> 3;
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+      const T2 *row = STAGED ? stage + r * (N / 2) : reinterpret_cast<const T2 *>(src + rowoff);
+      T2 v[N1];
+      sfor<0, N1>([&](auto J1) {
+        constexpr int j1 = SPM_CI(J1);
+        const int j = j1 * 8 + j2;
+        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : __ldg(row + j), acc);
+      });
+      Dft<-1, N1, T2>::run(v);
+      T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
+      sfor<0, N1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        E[k1] = (k1 == 0) ? v[k1] : cmul(v[k1], ztw[k1 * 8 + j2]);
+      });
+    }
+    __syncthreads();
+    if (STAGED && warp == 0 && next < N) {
+      fence_proxy_async();
+      issue(next);
+    }
+    // ---- z, stage 2: task (r, k1), 8-point DFT over j2 -> k = k1 + N1*k2
+    {
+      constexpr int NT = kRows * N1;
+      constexpr int TPT = (NT + kThreads - 1) / kThreads;
+      T2 u[TPT][8];
 #pragma unroll
-    for (int t = 0; t < TPT; t++) {
-      const int task = tid + t * kThreads;
-      if (task < NT) {
-        const int r = task / N1, k1 = task % N1;
+      for (int t = 0; t < TPT; t++) {
+        const int task = tid + t * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
 #pragma unroll
-        for (int j2 = 0; j2 < 8; j2++) u[t][j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          for (int j2 = 0; j2 < 8; j2++) u[t][j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int t = 0; t < TPT; t++) {
+        const int task = tid + t * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
+          Dft<-1, 8, T2>::run(u[t]);
+#pragma unroll
+          for (int k2 = 0; k2 < 8; k2++) buf[r * M + k1 + N1 * k2] = u[t][k2];
+        }
       }
     }
     __syncthreads();
-#pragma unroll
-    for (int t = 0; t < TPT; t++) {
-      const int task = tid + t * kThreads;
-      if (task < NT) {
-        const int r = task / N1, k1 = task % N1;
-        Dft<-1, 8, T2>::run(u[t]);
-#pragma unroll
-        for (int k2 = 0; k2 < 8; k2++) buf[r * M + k1 + N1 * k2] = u[t][k2];
+    // ---- z, real-to-complex post-processing of the packed line (pairs k, M-k)
+    {
+      constexpr int NT = kRows * (M / 2);
+      for (int task = tid; task < NT; task += kThreads) {
+        const int r = task / (M / 2), q = task % (M / 2);
+        T2 *Z = buf + r * M;
+        if (q == 0) {
+          const T2 z0 = Z[0];
+          Z[0] = T2{z0.x + z0.y, z0.x - z0.y};  // X_0 + i X_{N/2}
+          const T2 a = Z[M / 2];
+          const T2 e = {a.x, (T)0};            // (a + conj a)/2
+          const T2 o = {a.y, (T)0};            // (a - conj a)/(2i)
+          Z[M / 2] = cadd(e, cmul(tw[M / 2], o));
+        } else {
+          const T2 a = Z[q], c = Z[M - q];
+          const T2 e1 = {(T)0.5 * (a.x + c.x), (T)0.5 * (a.y - c.y)};  // (Z_q + conj Z_{M-q})/2
+          const T2 o1 = {(T)0.5 * (a.y + c.y), (T)0.5 * (c.x - a.x)};  // (Z_q - conj Z_{M-q})/(2i)
+          const T2 e2 = {e1.x, -e1.y};
+          const T2 o2 = {o1.x, -o1.y};
+          Z[q] = cadd(e1, cmul(tw[q], o1));
+          Z[M - q] = cadd(e2, cmul(tw[M - q], o2));
+        }
       }
     }
-  }
-  __syncthreads();
-  // ---- z, real-to-complex post-processing of the packed line (pairs k, M-k)
-  {
-    constexpr int NT = kRows * (M / 2);
-    for (int task = tid; task < NT; task += kThreads) {
-      const int r = task / (M / 2), q = task % (M / 2);
-      T2 *Z = buf + r * M;
-      if (q == 0) {
-        const T2 z0 = Z[0];
-        Z[0] = T2{z0.x + z0.y, z0.x - z0.y};  // X_0 + i X_{N/2}
-        const T2 a = Z[M / 2];
-        const T2 e = {a.x, (T)0};            // (a + conj a)/2
-        const T2 o = {a.y, (T)0};            // (a - conj a)/(2i)
-        Z[M / 2] = cadd(e, cmul(tw[M / 2], o));
-      } else {
-        const T2 a = Z[q], c = Z[M - q];
-        const T2 e1 = {(T)0.5 * (a.x + c.x), (T)0.5 * (a.y - c.y)};   // (Z_q + conj Z_{M-q})/2
-        const T2 o1 = {(T)0.5 * (a.y + c.y), (T)0.5 * (c.x - a.x)};   // (Z_q - conj Z_{M-q})/(2i)
-        const T2 e2 = {e1.x, -e1.y};
-        const T2 o2 = {o1.x, -o1.y};
-        Z[q] = cadd(e1, cmul(tw[q], o1));
-        Z[M - q] = cadd(e2, cmul(tw[M - q], o2));
-      }
-    }
-  }
-  cluster.sync();
-  // ---- y, stage 1: task (column c, j2); element y = 16*j1 + j2 lives in CTA y/32
-  {
-    const int c = tid & 15, j2 = tid >> 4;
-    const int col = rank * kCols + c;
-    T2 v[M1];
-    sfor<0, M1>([&](auto J1) {
-      constexpr int j1 = SPM_CI(J1);
-      const int y = 16 * j1 + j2;
-      const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
-      v[j1] = rem[(y & 31) * M + col];
-    });
     cluster.sync();
-    Dft<-1, M1, T2>::run(v);
-    sfor<0, M1>([&](auto K1) {
-      constexpr int k1 = SPM_CI(K1);
-      buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmul(v[k1], tw[j2 * k1]);
-    });
-  }
-  __syncthreads();
-  // ---- y, stage 2: task (c, k1) -> ky = k1 + M1*k2; write the spectral column
-  if (tid < 16 * M1) {
-    const int c = tid & 15, k1 = tid >> 4;
-    const int col = rank * kCols + c;
-    T2 u[16];
-#pragma unroll
-    for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
-    Dft<-1, 16, T2>::run(u);
-    T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
-#pragma unroll
-    for (int k2 = 0; k2 < 16; k2++) {
-      const int ky = k1 + M1 * k2;
-      dst[((size_t)plane * N + ky) * M + col] = u[k2];
+    // ---- y, stage 1: task (column c, j2); element y = 16*j1 + j2 lives in CTA y/32
+    {
+      const int c = tid & 15, j2 = tid >> 4;
+      const int col = rank * kCols + c;
+      T2 v[M1];
+      sfor<0, M1>([&](auto J1) {
+        constexpr int j1 = SPM_CI(J1);
+        const int y = 16 * j1 + j2;
+        const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
+        v[j1] = rem[(y & 31) * M + col];
+      });
+      cluster.sync();
+      Dft<-1, M1, T2>::run(v);
+      sfor<0, M1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmul(v[k1], tw[j2 * k1]);
+      });
     }
+    __syncthreads();
+    // ---- y, stage 2: task (c, k1) -> ky = k1 + M1*k2; write the spectral column
+    if (tid < 16 * M1) {
+      const int c = tid & 15, k1 = tid >> 4;
+      const int col = rank * kCols + c;
+      T2 u[16];
+#pragma unroll
+      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+      Dft<-1, 16, T2>::run(u);
+      T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; k2++) {
+        const int ky = k1 + M1 * k2;
+        dst[((size_t)plane * N + ky) * M + col] = u[k2];
+      }
+    }
+    __syncthreads();
   }
+  report_error(p, s_err);
   if constexpr (Pro::NR > 0) {
     double tot[Pro::NR];
     if (grid_reduce<Pro::NR, Pro::MAXM>(acc, red, p.partials + (size_t)b * kPartStride * kRedMax,
-                                        p.tickets + b, G::BLOCKS, blockIdx.x, tot))
+                                        p.tickets + b, gridDim.x, blockIdx.x, tot))
       Pro::fin(p, b, tot);
   }
 }
@@ -201,155 +245,182 @@ __global__ void __launch_bounds__(kThreads) plane_fwd_kernel(const __grid_consta
 //       f = unnormalised forward value, s = state value, w = multiplicity of the
 //       point in the full N^3 spectrum (1 on the kz = 0, N/2 planes, else 2).
 //     __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
+// Stages: [A (if FI)][S (if SI)], each 2 rows x N x 8 columns, [row][x][cc].
 template <int N, class T, class Op>
-__global__ void __launch_bounds__(kThreads) pencil_kernel(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
   constexpr int M = G::M, M1 = G::M1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
+  constexpr int NST = (Op::FI ? 1 : 0) + (Op::SI ? 1 : 0);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
   T2 *ex = tw + N;
-  double *red = reinterpret_cast<double *>(ex + G::PENCIL_UNITS);
+  T2 *sA = ex + G::PENCIL_UNITS;
+  T2 *sS = sA + (Op::FI ? G::STAGE_UNITS : 0);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ex + G::PENCIL_UNITS + NST * G::STAGE_UNITS);
+  double *red = reinterpret_cast<double *>(bars + 2);
+  __shared__ int s_err;
   if (flow_stopped(p)) return;
 
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
-  const int t = blockIdx.x % (N / 2);
-  const int c0 = (blockIdx.x / (N / 2)) * 8;
   const int pen = tid & 15, rowsel = pen >> 3, cc = pen & 7;
-  const int ky0 = t, ky1 = (t == 0) ? N / 2 : N - t;
-  const int ky = rowsel ? ky1 : ky0;
-  const int col = c0 + cc;
-  const bool dc = (c0 == 0);
   const bool has2 = (tid >> 4) < M1;  // owns a stage-2 task (pencil, k1)
   const int k1 = tid >> 4;
+  // Tiles run columns-fastest, so concurrently resident CTAs read adjacent
+  // 8-column segments of the same ky rows.
+  constexpr int NCH = M / 8;
+  // thread 0: two tensor boxes (8 columns x all x) for rows ky0, ky1 of a tile
+  auto issue = [&](const CUtensorMap *map, T2 *dst, uint64_t *bar, int tile) {
+    const int t = tile / NCH, c0 = (tile % NCH) * 8;
+    const int ky0 = t, ky1 = (t == 0) ? N / 2 : N - t;
+    mbar_expect_tx(bar, (unsigned)(2 * N * 8 * sizeof(T2)));
+    tma_load_3d(dst, map, 2 * c0, ky0, 0, bar);
+    tma_load_3d(dst + N * 8, map, 2 * c0, ky1, 0, bar);
+  };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    s_err = 0;
+    fence_barrier_init();
+  }
   for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
   double acc[Op::NR > 0 ? Op::NR : 1];
 #pragma unroll
   for (int r = 0; r < (Op::NR > 0 ? Op::NR : 1); r++) acc[r] = ((Op::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
   __syncthreads();
+  int tile = blockIdx.x;
+  if (tid == 0 && tile < G::PTILES) {
+    if (Op::FI) issue(&p.tmi[b], sA, &bars[0], tile);
+    if (Op::SI) issue(&p.tms[b], sS, &bars[1], tile);
+  }
 
-  T2 F[16], S[16];
-  if constexpr (Op::FI) {
-    // stage 1: task (pencil, j2 = tid/16): x = 16*j1 + j2
-    {
-      const int j2 = tid >> 4;
-      const T2 *src = reinterpret_cast<const T2 *>(p.in[b]);
-      T2 v[M1];
-      sfor<0, M1>([&](auto J1) {
-        constexpr int j1 = SPM_CI(J1);
-        const int x = 16 * j1 + j2;
-        v[j1] = __ldg(src + ((size_t)x * N + ky) * M + col);
-      });
-      Dft<-1, M1, T2>::run(v);
-      sfor<0, M1>([&](auto K1) {
-        constexpr int kk = SPM_CI(K1);
-        ex[kk * 256 + j2 * 16 + pen] = (kk == 0) ? v[kk] : cmul(v[kk], tw[j2 * kk]);
-      });
-    }
-    __syncthreads();
-    if (has2) {
-#pragma unroll
-      for (int j2 = 0; j2 < 16; j2++) F[j2] = ex[k1 * 256 + j2 * 16 + pen];
-      Dft<-1, 16, T2>::run(F);  // F[k2] at kx = k1 + M1*k2
-    }
-  }
-  if constexpr (Op::SI) {
-    if (has2) {
-      const T2 *st = reinterpret_cast<const T2 *>(p.st[b]);
-#pragma unroll
-      for (int k2 = 0; k2 < 16; k2++) S[k2] = st[((size_t)(k1 + M1 * k2) * N + ky) * M + col];
-    }
-  }
-  // partner values at (-kx, -ky) for the packed c = 0 pencils
-  T2 Fp[16], Sp[16];
-  if constexpr (!Op::LIN) {
-    if (dc) {
-      __syncthreads();
-      T2 *D = ex;  // [quantity][rowsel][kx]
-      if (has2 && cc == 0) {
-#pragma unroll
-        for (int k2 = 0; k2 < 16; k2++) {
-          const int kx = k1 + M1 * k2;
-          if constexpr (Op::FI) D[(0 * 2 + rowsel) * N + kx] = F[k2];
-          if constexpr (Op::SI) D[(1 * 2 + rowsel) * N + kx] = S[k2];
-        }
+  for (int it = 0; tile < G::PTILES; tile += gridDim.x, it++) {
+    const int next = tile + gridDim.x;
+    const int t = tile / NCH;
+    const int c0 = (tile % NCH) * 8;
+    const int ky0 = t, ky1 = (t == 0) ? N / 2 : N - t;
+    const int ky = rowsel ? ky1 : ky0;
+    const int col = c0 + cc;
+    const bool dc = (c0 == 0);
+
+    T2 F[16];
+    if constexpr (Op::FI) {
+      mbar_wait(&bars[0], it & 1, &s_err);
+      {  // stage 1: task (pencil, j2 = tid/16): x = 16*j1 + j2
+        const int j2 = tid >> 4;
+        T2 v[M1];
+        sfor<0, M1>([&](auto J1) {
+          constexpr int j1 = SPM_CI(J1);
+          v[j1] = sA[(rowsel * N + 16 * j1 + j2) * 8 + cc];
+        });
+        Dft<-1, M1, T2>::run(v);
+        sfor<0, M1>([&](auto K1) {
+          constexpr int kk = SPM_CI(K1);
+          ex[kk * 256 + j2 * 16 + pen] = (kk == 0) ? v[kk] : cmul(v[kk], tw[j2 * kk]);
+        });
       }
       __syncthreads();
-      if (has2 && cc == 0) {
-        const int pr = (t == 0) ? rowsel : 1 - rowsel;
+      if (tid == 0 && next < G::PTILES) {
+        fence_proxy_async();
+        issue(&p.tmi[b], sA, &bars[0], next);
+      }
+      if (has2) {
 #pragma unroll
-        for (int k2 = 0; k2 < 16; k2++) {
-          const int kx = k1 + M1 * k2;
+        for (int j2 = 0; j2 < 16; j2++) F[j2] = ex[k1 * 256 + j2 * 16 + pen];
+        Dft<-1, 16, T2>::run(F);  // F[k2] at kx = k1 + M1*k2
+      }
+    }
+    if constexpr (Op::SI) mbar_wait(&bars[1], it & 1, &s_err);
+    // partner values at (-kx, -ky) for the packed c = 0 pencils, through ex
+    if constexpr (!Op::LIN) {
+      if (dc) {
+        __syncthreads();
+        T2 *D = ex;  // [quantity][rowsel][kx]
+        if (has2 && cc == 0) {
+#pragma unroll
+          for (int k2 = 0; k2 < 16; k2++) {
+            const int kx = k1 + M1 * k2;
+            if constexpr (Op::FI) D[(0 * 2 + rowsel) * N + kx] = F[k2];
+            if constexpr (Op::SI) D[(1 * 2 + rowsel) * N + kx] = sS[(rowsel * N + kx) * 8];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // the per-point operator
+    if (has2) {
+      T2 *so = Op::SO ? reinterpret_cast<T2 *>(p.sto[b]) : nullptr;
+      const int Ky = wave(ky, N);
+      const int pr = (t == 0) ? rowsel : 1 - rowsel;
+#pragma unroll
+      for (int k2 = 0; k2 < 16; k2++) {
+        const int kx = k1 + M1 * k2;
+        const int Kx = wave(kx, N);
+        const T2 f = Op::FI ? F[k2] : T2{0, 0};
+        const T2 s = Op::SI ? sS[(rowsel * N + kx) * 8 + cc] : T2{0, 0};
+        T2 o_st = {0, 0}, o_inv = {0, 0};
+        if (!Op::LIN && dc && cc == 0) {
+          // unpack X(., ., 0) and X(., ., N/2), apply, repack
           const int nk = kx ? N - kx : 0;
-          if constexpr (Op::FI) Fp[k2] = D[(0 * 2 + pr) * N + nk];
-          if constexpr (Op::SI) Sp[k2] = D[(1 * 2 + pr) * N + nk];
+          T2 f0 = {0, 0}, fM = {0, 0}, s0 = {0, 0}, sM = {0, 0};
+          if constexpr (Op::FI) {
+            const T2 q = ex[(0 * 2 + pr) * N + nk];
+            f0 = T2{(T)0.5 * (f.x + q.x), (T)0.5 * (f.y - q.y)};
+            fM = T2{(T)0.5 * (f.y + q.y), (T)0.5 * (q.x - f.x)};
+          }
+          if constexpr (Op::SI) {
+            const T2 q = ex[(1 * 2 + pr) * N + nk];
+            s0 = T2{(T)0.5 * (s.x + q.x), (T)0.5 * (s.y - q.y)};
+            sM = T2{(T)0.5 * (s.y + q.y), (T)0.5 * (q.x - s.x)};
+          }
+          T2 so0, inv0, soM, invM;
+          Op::point(p, b, Kx, Ky, 0, f0, s0, so0, inv0, acc, 1.0);
+          Op::point(p, b, Kx, Ky, -N / 2, fM, sM, soM, invM, acc, 1.0);
+          o_st = T2{so0.x - soM.y, so0.y + soM.x};
+          o_inv = T2{inv0.x - invM.y, inv0.y + invM.x};
+        } else {
+          Op::point(p, b, Kx, Ky, col, f, s, o_st, o_inv, acc, dc && cc == 0 ? 1.0 : 2.0);
         }
+        if constexpr (Op::SO) so[((size_t)kx * N + ky) * M + col] = o_st;
+        F[k2] = o_inv;
       }
     }
-  }
-  // the per-point operator
-  if (has2) {
-    T2 *so = Op::SO ? reinterpret_cast<T2 *>(p.sto[b]) : nullptr;
-    const int Ky = wave(ky, N);
-#pragma unroll
-    for (int k2 = 0; k2 < 16; k2++) {
-      const int kx = k1 + M1 * k2;
-      const int Kx = wave(kx, N);
-      T2 f = Op::FI ? F[k2] : T2{0, 0};
-      T2 s = Op::SI ? S[k2] : T2{0, 0};
-      T2 o_st = {0, 0}, o_inv = {0, 0};
-      if (!Op::LIN && dc && cc == 0) {
-        // unpack X(., ., 0) and X(., ., N/2), apply, repack
-        T2 f0 = {0, 0}, fM = {0, 0}, s0 = {0, 0}, sM = {0, 0};
-        if constexpr (Op::FI) {
-          const T2 q = Fp[k2];
-          f0 = T2{(T)0.5 * (f.x + q.x), (T)0.5 * (f.y - q.y)};
-          fM = T2{(T)0.5 * (f.y + q.y), (T)0.5 * (q.x - f.x)};
-        }
-        if constexpr (Op::SI) {
-          const T2 q = Sp[k2];
-          s0 = T2{(T)0.5 * (s.x + q.x), (T)0.5 * (s.y - q.y)};
-          sM = T2{(T)0.5 * (s.y + q.y), (T)0.5 * (q.x - s.x)};
-        }
-        T2 so0, inv0, soM, invM;
-        Op::point(p, b, Kx, Ky, 0, f0, s0, so0, inv0, acc, 1.0);
-        Op::point(p, b, Kx, Ky, -N / 2, fM, sM, soM, invM, acc, 1.0);
-        o_st = T2{so0.x - soM.y, so0.y + soM.x};
-        o_inv = T2{inv0.x - invM.y, inv0.y + invM.x};
-      } else {
-        Op::point(p, b, Kx, Ky, col, f, s, o_st, o_inv, acc, dc && cc == 0 ? 1.0 : 2.0);
+    __syncthreads();  // sS and ex reads done
+    if constexpr (Op::SI) {
+      if (tid == 0 && next < G::PTILES) {
+        fence_proxy_async();
+        issue(&p.tms[b], sS, &bars[1], next);
       }
-      if constexpr (Op::SO) so[((size_t)kx * N + ky) * M + col] = o_st;
-      F[k2] = o_inv;
     }
-  }
-  if constexpr (Op::INV) {
-    __syncthreads();
-    if (has2) {
-      Dft<+1, 16, T2>::run(F);  // over k2 -> j2
+    if constexpr (Op::INV) {
+      if (has2) {
+        Dft<+1, 16, T2>::run(F);  // over k2 -> j2
 #pragma unroll
-      for (int j2 = 0; j2 < 16; j2++)
-        ex[k1 * 256 + j2 * 16 + pen] = (j2 == 0 || k1 == 0) ? F[j2] : cmulc(F[j2], tw[j2 * k1]);
-    }
-    __syncthreads();
-    {
-      const int j2 = tid >> 4;
-      T2 v[M1];
-      sfor<0, M1>([&](auto K1) { v[SPM_CI(K1)] = ex[SPM_CI(K1) * 256 + j2 * 16 + pen]; });
-      Dft<+1, M1, T2>::run(v);
-      T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
-      sfor<0, M1>([&](auto J1) {
-        constexpr int j1 = SPM_CI(J1);
-        const int x = 16 * j1 + j2;
-        dst[((size_t)x * N + ky) * M + col] = v[j1];
-      });
+        for (int j2 = 0; j2 < 16; j2++)
+          ex[k1 * 256 + j2 * 16 + pen] = (j2 == 0 || k1 == 0) ? F[j2] : cmulc(F[j2], tw[j2 * k1]);
+      }
+      __syncthreads();
+      {
+        const int j2 = tid >> 4;
+        T2 v[M1];
+        sfor<0, M1>([&](auto K1) { v[SPM_CI(K1)] = ex[SPM_CI(K1) * 256 + j2 * 16 + pen]; });
+        Dft<+1, M1, T2>::run(v);
+        T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
+        sfor<0, M1>([&](auto J1) {
+          constexpr int j1 = SPM_CI(J1);
+          const int x = 16 * j1 + j2;
+          dst[((size_t)x * N + ky) * M + col] = v[j1];
+        });
+      }
+      __syncthreads();
     }
   }
+  report_error(p, s_err);
   if constexpr (Op::NR > 0) {
     double tot[Op::NR];
     if (grid_reduce<Op::NR, Op::MAXM>(acc, red, p.partials + (size_t)b * kPartStride * kRedMax,
-                                      p.tickets + b, G::PBLOCKS, blockIdx.x, tot))
+                                      p.tickets + b, gridDim.x, blockIdx.x, tot))
       Op::fin(p, b, tot);
   }
 }
@@ -359,154 +430,184 @@ __global__ void __launch_bounds__(kThreads) pencil_kernel(const __grid_constant_
 //      __device__ static T2 epi(const KParams&, int b, size_t idx, T2 y, double (&acc)[NR]);
 //        (y = unnormalised inverse transform at reals idx, idx+1; returns values to store)
 //      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
-template <int N, class T, class Epi>
-__global__ void __launch_bounds__(kThreads) plane_inv_kernel(const __grid_constant__ KParams p) {
+// CPS as for plane_fwd: 1 stages the next plane's columns with a tensor copy,
+// 2 loads them straight from global memory (two CTAs per SM).
+template <int N, class T, class Epi, int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
   constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + N;
-  double *red = reinterpret_cast<double *>(buf + G::PLANE_UNITS);
+  constexpr bool STAGED = (CPS == 1);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
+  T2 *ztw = tw + N;
+  T2 *buf = ztw + N / 2;
+  T2 *stage = buf + G::PLANE_UNITS;  // [ky][16 columns]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
+  double *red = reinterpret_cast<double *>(bar + 2);
+  __shared__ int s_err;
   if (flow_stopped(p)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
-  const int plane = blockIdx.x / G::CL;
+  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  auto issue = [&](int plane) {  // thread 0: one tensor box (this CTA's 16 columns x all ky)
+    mbar_expect_tx(bar, (unsigned)(N * 16 * sizeof(T2)));
+    tma_load_3d(stage, &p.tmi[b], 2 * rank * kCols, 0, plane, bar);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    s_err = 0;
+    fence_barrier_init();
+  }
   for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
+  __syncthreads();
+  for (int i = tid; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
   double acc[Epi::NR > 0 ? Epi::NR : 1];
 #pragma unroll
   for (int r = 0; r < (Epi::NR > 0 ? Epi::NR : 1); r++) acc[r] = ((Epi::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  int plane = cid;
+  if (STAGED && tid == 0 && plane < N) issue(plane);
   __syncthreads();
+  const T2 *gsrc = reinterpret_cast<const T2 *>(p.in[b]);
 
-  // ---- inverse y, stage 1: task (c, j2), input ky = 16*j1 + j2 (natural order)
-  {
-    const int c = tid & 15, j2 = tid >> 4;
-    const int col = rank * kCols + c;
-    const T2 *src = reinterpret_cast<const T2 *>(p.in[b]);
-    T2 v[M1];
-    sfor<0, M1>([&](auto J1) {
-      constexpr int j1 = SPM_CI(J1);
-      v[j1] = __ldg(src + ((size_t)plane * N + (16 * j1 + j2)) * M + col);
-    });
-    Dft<+1, M1, T2>::run(v);
-    sfor<0, M1>([&](auto K1) {
-      constexpr int k1 = SPM_CI(K1);
-      buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
-    });
-  }
-  __syncthreads();
-  // ---- inverse y, stage 2: task (c, k1) -> y = k1 + M1*k2; keep [y][c] in smem
-  {
-    T2 u[16];
-    const int c = tid & 15, k1 = tid >> 4;
-    if (tid < 16 * M1) {
-#pragma unroll
-      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
-      Dft<+1, 16, T2>::run(u);
+  for (int it = 0; plane < N; plane += ncl, it++) {
+    const int next = plane + ncl;
+    if (STAGED) mbar_wait(bar, it & 1, &s_err);
+    // ---- inverse y, stage 1: task (c, j2), input ky = 16*j1 + j2 (natural order)
+    {
+      const int c = tid & 15, j2 = tid >> 4;
+      T2 v[M1];
+      sfor<0, M1>([&](auto J1) {
+        constexpr int j1 = SPM_CI(J1);
+        v[j1] = STAGED ? stage[(16 * j1 + j2) * 16 + c]
+                       : __ldg(gsrc + ((size_t)plane * N + (16 * j1 + j2)) * M + rank * kCols + c);
+      });
+      Dft<+1, M1, T2>::run(v);
+      sfor<0, M1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
+      });
     }
     __syncthreads();
-    if (tid < 16 * M1) {
-#pragma unroll
-      for (int k2 = 0; k2 < 16; k2++) buf[(k1 + M1 * k2) * 16 + c] = u[k2];
+    if (STAGED && tid == 0 && next < N) {
+      fence_proxy_async();
+      issue(next);
     }
-  }
-  cluster.sync();
-  // ---- complex-to-real pre-processing: gather the pairs (q, M-q) of my rows
-  {
-    constexpr int NT = kRows * (M / 2);
-    constexpr int TPT = NT / kThreads;  // N/32 tasks per thread
-    static_assert(NT % kThreads == 0, "task count");
-    T2 za[TPT], zb[TPT];
+    // ---- inverse y, stage 2: task (c, k1) -> y = k1 + M1*k2; keep [y][c] in smem
+    {
+      T2 u[16];
+      const int c = tid & 15, k1 = tid >> 4;
+      if (tid < 16 * M1) {
 #pragma unroll
-    for (int i = 0; i < TPT; i++) {
-      const int task = tid + i * kThreads;
-      const int r = task / (M / 2), q = task % (M / 2);
-      const int y = rank * kRows + r;
-      if (q == 0) {
-        const T2 *r0 = cluster.map_shared_rank(buf, 0u);
-        const T2 *rh = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols));
-        const T2 P = r0[y * 16 + 0];
-        const T2 a = rh[y * 16 + (M / 2) % kCols];
-        // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
-        za[i] = T2{P.x + P.y, P.x - P.y};
-        // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
-        const T2 e = {a.x + a.x, (T)0};
-        const T2 o = {(T)0, a.y + a.y};
-        zb[i] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
-      } else {
-        const T2 *ra = cluster.map_shared_rank(buf, (unsigned)(q / kCols));
-        const T2 *rb = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols));
-        const T2 a = ra[y * 16 + q % kCols];
-        const T2 c = rb[y * 16 + (M - q) % kCols];
-        // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
-        const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
-        const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
-        za[i] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
-        zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
+        for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+        Dft<+1, 16, T2>::run(u);
+      }
+      __syncthreads();
+      if (tid < 16 * M1) {
+#pragma unroll
+        for (int k2 = 0; k2 < 16; k2++) buf[(k1 + M1 * k2) * 16 + c] = u[k2];
       }
     }
     cluster.sync();
+    // ---- complex-to-real pre-processing: gather the pairs (q, M-q) of my rows
+    {
+      constexpr int NT = kRows * (M / 2);
+      constexpr int TPT = NT / kThreads;  // N/32 tasks per thread
+      static_assert(NT % kThreads == 0, "task count");
+      T2 za[TPT], zb[TPT];
 #pragma unroll
-    for (int i = 0; i < TPT; i++) {
-      const int task = tid + i * kThreads;
-      const int r = task / (M / 2), q = task % (M / 2);
-      T2 *Z = buf + r * M;
-      if (q == 0) {
-        Z[0] = za[i];
-        Z[M / 2] = zb[i];
-      } else {
-        Z[q] = za[i];
-        Z[M - q] = zb[i];
+      for (int i = 0; i < TPT; i++) {
+        const int task = tid + i * kThreads;
+        const int r = task / (M / 2), q = task % (M / 2);
+        const int y = rank * kRows + r;
+        if (q == 0) {
+          const T2 *r0 = cluster.map_shared_rank(buf, 0u);
+          const T2 *rh = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols));
+          const T2 P = r0[y * 16 + 0];
+          const T2 a = rh[y * 16 + (M / 2) % kCols];
+          // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
+          za[i] = T2{P.x + P.y, P.x - P.y};
+          // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
+          const T2 e = {a.x + a.x, (T)0};
+          const T2 o = {(T)0, a.y + a.y};
+          zb[i] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
+        } else {
+          const T2 *ra = cluster.map_shared_rank(buf, (unsigned)(q / kCols));
+          const T2 *rb = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols));
+          const T2 a = ra[y * 16 + q % kCols];
+          const T2 c = rb[y * 16 + (M - q) % kCols];
+          // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
+          const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
+          const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
+          za[i] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
+          zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
+        }
       }
-    }
-  }
-  __syncthreads();
-  // ---- inverse z, stage 1: task (r, j2), element j = j1*8 + j2
-  {
-    const int j2 = tid & 7, r = tid >> 3;
-    T2 v[N1];
-    sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
-    __syncthreads();
-    Dft<+1, N1, T2>::run(v);
-    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
-    sfor<0, N1>([&](auto K1) {
-      constexpr int k1 = SPM_CI(K1);
-      E[k1] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[2 * j2 * k1]);
-    });
-  }
-  __syncthreads();
-  // ---- inverse z, stage 2: task (r, k1) -> j = k1 + N1*k2; z_j = y_{2j} + i y_{2j+1}
-  {
-    constexpr int NT = kRows * N1;
-    constexpr int TPT = (NT + kThreads - 1) / kThreads;
+      cluster.sync();
 #pragma unroll
-    for (int t2 = 0; t2 < TPT; t2++) {
-      const int task = tid + t2 * kThreads;
-      if (task < NT) {
-        const int r = task / N1, k1 = task % N1;
-        T2 u[8];
-#pragma unroll
-        for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
-        Dft<+1, 8, T2>::run(u);
-        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
-        T *outb = reinterpret_cast<T *>(p.out[b]);  // null: reductions only
-        T2 *dst = reinterpret_cast<T2 *>(outb + rowoff);
-#pragma unroll
-        for (int k2 = 0; k2 < 8; k2++) {
-          const int j = k1 + N1 * k2;
-          const T2 val = Epi::epi(p, b, rowoff + 2 * j, u[k2], acc);
-          if (outb) dst[j] = val;
+      for (int i = 0; i < TPT; i++) {
+        const int task = tid + i * kThreads;
+        const int r = task / (M / 2), q = task % (M / 2);
+        T2 *Z = buf + r * M;
+        if (q == 0) {
+          Z[0] = za[i];
+          Z[M / 2] = zb[i];
+        } else {
+          Z[q] = za[i];
+          Z[M - q] = zb[i];
         }
       }
     }
+    __syncthreads();
+    // ---- inverse z, stage 1: task (r, j2), element j = j1*8 + j2
+    {
+      const int j2 = tid & 7, r = tid >> 3;
+      T2 v[N1];
+      sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
+      __syncthreads();
+      Dft<+1, N1, T2>::run(v);
+      T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
+      sfor<0, N1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        E[k1] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
+      });
+    }
+    __syncthreads();
+    // ---- inverse z, stage 2: task (r, k1) -> j = k1 + N1*k2; z_j = y_{2j} + i y_{2j+1}
+    {
+      constexpr int NT = kRows * N1;
+      constexpr int TPT = (NT + kThreads - 1) / kThreads;
+#pragma unroll
+      for (int t2 = 0; t2 < TPT; t2++) {
+        const int task = tid + t2 * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
+          T2 u[8];
+#pragma unroll
+          for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          Dft<+1, 8, T2>::run(u);
+          const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+          T *outb = reinterpret_cast<T *>(p.out[b]);  // null: reductions only
+          T2 *dst = reinterpret_cast<T2 *>(outb + rowoff);
+#pragma unroll
+          for (int k2 = 0; k2 < 8; k2++) {
+            const int j = k1 + N1 * k2;
+            const T2 val = Epi::epi(p, b, rowoff + 2 * j, u[k2], acc);
+            if (outb) dst[j] = val;
+          }
+        }
+      }
+    }
+    __syncthreads();
   }
+  report_error(p, s_err);
   if constexpr (Epi::NR > 0) {
     double tot[Epi::NR];
     if (grid_reduce<Epi::NR, Epi::MAXM>(acc, red, p.partials + (size_t)b * kPartStride * kRedMax,
-                                        p.tickets + b, G::BLOCKS, blockIdx.x, tot))
+                                        p.tickets + b, gridDim.x, blockIdx.x, tot))
       Epi::fin(p, b, tot);
   }
 }

@@ -18,25 +18,25 @@ template <class T> struct ProIdent {
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
 };
 
-// Gradient step (LPsrc.cpp:44-75): transform f = Tau u + Gamma u^2 - u^3 and sum
-// the local energy density -Tau/2 u^2 - Gamma/3 u^3 + u^4/4 (LPsrc.cpp:10-24).
+// Local polynomials of the model in Horner form (a few ulp from the
+// reference's term-by-term order, LPsrc.cpp:10-24, 58-62):
+//   nonlinear force  f(u) = Tau u + Gamma u^2 - u^3 = u (Tau + u (Gamma - u))
+//   energy density   e(u) = -Tau/2 u^2 - Gamma/3 u^3 + u^4/4
+//                         = u^2 (-Tau/2 + u (-Gamma/3 + u/4))
+template <class T> __device__ __forceinline__ T poly_force(T u, T tau, T gam) { return u * (tau + u * (gam - u)); }
+template <class T> __device__ __forceinline__ T poly_energy(T u, T mtau2, T mgam3) {
+  return (u * u) * (mtau2 + u * (mgam3 + (T)0.25 * u));
+}
+
+// Gradient step (LPsrc.cpp:44-75): transform f(u) and sum the energy density.
 template <class T> struct ProGrad {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
   __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, double (&acc)[1]) {
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
-    c2<T> f;
-    {
-      const T u = x.x, u2 = u * u, u3 = u2 * u, u4 = u3 * u;
-      acc[0] += (double)(-(T)0.5 * tau * u2 - gam * u3 / (T)3 + (T)0.25 * u4);
-      f.x = tau * u + gam * u2 - u3;
-    }
-    {
-      const T u = x.y, u2 = u * u, u3 = u2 * u, u4 = u3 * u;
-      acc[0] += (double)(-(T)0.5 * tau * u2 - gam * u3 / (T)3 + (T)0.25 * u4);
-      f.y = tau * u + gam * u2 - u3;
-    }
-    return f;
+    const T mtau2 = (T)(-0.5 * p.m.Tau), mgam3 = (T)(-p.m.Gamma / 3.0);
+    acc[0] += (double)poly_energy(x.x, mtau2, mgam3) + (double)poly_energy(x.y, mtau2, mgam3);
+    return c2<T>{poly_force(x.x, tau, gam), poly_force(x.y, tau, gam)};
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
     scal_of(p, b)[SC_E2] = tot[0] * p.m.inv_n3;
@@ -70,8 +70,7 @@ template <class T> struct ProNgrad {
   static constexpr unsigned MAXM = 0;
   __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, double (&acc)[1]) {
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
-    acc[0] += (double)(tau * x.x + gam * x.x * x.x - x.x * x.x * x.x);
-    acc[0] += (double)(tau * x.y + gam * x.y * x.y - x.y * x.y * x.y);
+    acc[0] += (double)poly_force(x.x, tau, gam) + (double)poly_force(x.y, tau, gam);
     return x;
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
@@ -106,8 +105,8 @@ template <class T> struct ProForce {
     const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
     const c2<T> gv = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
-    const T n0 = tau * x.x + gam * x.x * x.x - x.x * x.x * x.x;
-    const T n1 = tau * x.y + gam * x.y * x.y - x.y * x.y * x.y;
+    const T n0 = poly_force(x.x, tau, gam);
+    const T n1 = poly_force(x.y, tau, gam);
     acc[0] += (double)x.x * (double)gv.x + (double)x.y * (double)gv.y;
     acc[1] += (double)n0 * (double)v.x + (double)n1 * (double)v.y;
     acc[2] += (double)n0 + (double)n1;
@@ -172,12 +171,12 @@ template <class T> struct OpGrad {
   static constexpr unsigned MAXM = 0x2;
   __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &so,
                                c2<T> &inv, double (&acc)[3], double w) {
-    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
-    const T Gt = (T)G;
+    const double4 sy = symbols(p, Kx, Ky, Kz);
+    const double G = sy.x;
     const T dt = (T)p.m.dt;
     const c2<T> fh = cscale(f, (T)p.m.inv_n3);
-    const T den = (T)1 + dt * Gt;
-    c2<T> u1 = {(dt * fh.x + s.x) / den, (dt * fh.y + s.y) / den};
+    const T iden = (T)sy.y;  // 1 / (1 + dt G)
+    c2<T> u1 = {(dt * fh.x + s.x) * iden, (dt * fh.y + s.y) * iden};
     const bool k0 = (Kx == 0 && Ky == 0 && Kz == 0);
     if (k0) u1 = c2<T>{0, 0};
     acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
@@ -220,7 +219,7 @@ template <class T, bool ZERO_DC> struct OpGmul {
   static constexpr unsigned MAXM = 0;
   __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const T g = (T)gk_of(Kx, Ky, Kz, p.m.invL);
+    const T g = (T)symbols(p, Kx, Ky, Kz).x;
     inv = cscale(cscale(f, (T)p.m.inv_n3), g);
     if (ZERO_DC && Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
   }
@@ -234,8 +233,7 @@ template <class T> struct OpPrecond {
   static constexpr unsigned MAXM = 0;
   __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
-    const T ik = (T)(1.0 / (G + fabs(p.m.Tau) + 0.02));
+    const T ik = (T)symbols(p, Kx, Ky, Kz).z;  // 1 / (G + |Tau| + 0.02)
     inv = cscale(cscale(f, (T)p.m.inv_n3), ik);
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -250,11 +248,10 @@ template <class T> struct OpForce {
   static constexpr unsigned MAXM = 0;
   __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    const T iden = (T)symbols(p, Kx, Ky, Kz).w;  // 1 / (1 + G)
     const T sc = (T)scal_of(p, b)[SC_S];
-    const T den = (T)1 + (T)G;
     const c2<T> fh = cscale(f, (T)p.m.inv_n3);
-    inv = c2<T>{(fh.x - sc * s.x) / den, (fh.y - sc * s.y) / den};
+    inv = c2<T>{(fh.x - sc * s.x) * iden, (fh.y - sc * s.y) * iden};
     if (Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -272,7 +269,7 @@ template <class T, bool NORM = true> struct OpTangent {
     const T inrm = NORM ? (T)(1.0 / sqrt(scal_of(p, b)[SC_NRM2])) : (T)1;
     const c2<T> v = cscale(cscale(f, (T)p.m.inv_n3), inrm);
     so = v;
-    const T g = (T)gk_of(Kx, Ky, Kz, p.m.invL);
+    const T g = (T)symbols(p, Kx, Ky, Kz).x;
     inv = (Kx == 0 && Ky == 0 && Kz == 0) ? c2<T>{0, 0} : cscale(v, g);
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -285,7 +282,7 @@ template <class T> struct OpE1 {
   static constexpr unsigned MAXM = 0;
   __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T>, c2<T> s, c2<T> &, c2<T> &,
                                double (&acc)[1], double w) {
-    const double G = gk_of(Kx, Ky, Kz, p.m.invL);
+    const double G = symbols(p, Kx, Ky, Kz).x;
     acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {

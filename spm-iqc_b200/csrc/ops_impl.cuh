@@ -25,12 +25,13 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
   return e;
 }
 
+// Persistent cluster launch: as many clusters as can be resident at once
+// (queried once per kernel and device), at most one per x-plane.
 template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p,
                                                                int nb, const char *what) {
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, what);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(Geo<N>::BLOCKS, nb, 1);
   cfg.blockDim = dim3(kThreads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = c->stream;
@@ -41,27 +42,65 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
+  static int ncl[32] = {0};
+  const int dev = c->device < 32 ? c->device : 0;
+  if (ncl[dev] == 0) {
+    cfg.gridDim = dim3(Geo<N>::CL * N, 1, 1);
+    int n = 0;
+    e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
+    if (e != cudaSuccess || n < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, what);
+    ncl[dev] = n < N ? n : N;
+  }
+  cfg.gridDim = dim3(Geo<N>::CL * ncl[dev], nb, 1);
   c->launches++;
   e = cudaLaunchKernelEx(&cfg, kern, p);
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, what);
 }
 
+// The plane kernels come in two variants (c->plane_cps): 1 = staged, one CTA
+// per SM; 2 = direct loads, two CTAs per SM.
 template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
-  struct Tag {};
-  return launch_cluster<Tag, N>(c, plane_fwd_kernel<N, T, Pro>, plane_smem<N, T>(), p, nb, "plane_fwd");
+  if (c->plane_cps == 2) {
+    struct Tag2 {};
+    return launch_cluster<Tag2, N>(c, plane_fwd_kernel<N, T, Pro, 2>, plane_smem<N, T, 2>(), p, nb, "plane_fwd");
+  }
+  struct Tag1 {};
+  return launch_cluster<Tag1, N>(c, plane_fwd_kernel<N, T, Pro, 1>, plane_smem<N, T, 1>(), p, nb, "plane_fwd");
 }
-template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p, int nb) {
-  struct Tag {};
-  return launch_cluster<Tag, N>(c, plane_inv_kernel<N, T, Epi>, plane_smem<N, T>(), p, nb, "plane_inv");
+template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p0, int nb) {
+  if (c->plane_cps == 2) {
+    struct Tag2 {};
+    return launch_cluster<Tag2, N>(c, plane_inv_kernel<N, T, Epi, 2>, plane_smem<N, T, 2>(), p0, nb, "plane_inv");
+  }
+  struct Tag1 {};
+  KParams p = p0;
+  for (int b = 0; b < nb; b++) SPM_TRY(spm_tensor_map(c, p.in[b], TM_PLANE_INV, &p.tmi[b]));
+  return launch_cluster<Tag1, N>(c, plane_inv_kernel<N, T, Epi, 1>, plane_smem<N, T, 1>(), p, nb, "plane_inv");
 }
-template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p, int nb) {
+// Persistent pencil launch: resident CTAs (queried once), at most one per tile.
+template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p0, int nb) {
+  KParams p = p0;
+  for (int b = 0; b < nb; b++) {
+    if (Op::FI) SPM_TRY(spm_tensor_map(c, p.in[b], TM_PENCIL, &p.tmi[b]));
+    if (Op::SI) SPM_TRY(spm_tensor_map(c, p.st[b], TM_PENCIL, &p.tms[b]));
+  }
   auto kern = pencil_kernel<N, T, Op>;
-  constexpr size_t smem = pencil_smem<N, T>();
+  constexpr size_t smem = pencil_smem<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0));
   struct Tag {};
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, "pencil attribute");
+  static int nblk[32] = {0};
+  const int dev = c->device < 32 ? c->device : 0;
+  if (nblk[dev] == 0) {
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (e != cudaSuccess || per_sm < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration,
+                                                             "pencil occupancy");
+    nblk[dev] = per_sm * sms < Geo<N>::PTILES ? per_sm * sms : Geo<N>::PTILES;
+  }
   c->launches++;
-  kern<<<dim3(Geo<N>::PBLOCKS, nb, 1), kThreads, smem, c->stream>>>(p);
+  kern<<<dim3(nblk[dev], nb, 1), kThreads, smem, c->stream>>>(p);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, "pencil launch");
 }

@@ -1,10 +1,12 @@
 // Host side of the C ABI (include/spmiqc.h): contexts, scratch, launches and
 // the chains of kernels that make up each reference routine.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -79,6 +81,8 @@ KParams spm_params(const spm_ctx *c) {
   p.tickets = c->tickets;
   p.scal = c->scal;
   p.flow = c->gate;
+  p.gtab = reinterpret_cast<const double4 *>(c->gtab);
+  p.err = c->flow + FW_ERR;
   return p;
 }
 
@@ -104,12 +108,76 @@ int spm_ensure_scratch(spm_ctx *c, int nb) {
 char *spm_bufA(spm_ctx *c, int b) { return (char *)c->bufA + c->field_bytes * (size_t)b; }
 char *spm_bufB(spm_ctx *c, int b) { return (char *)c->bufB + c->field_bytes * (size_t)b; }
 
+// ------------------------------------------------------------------ tensor maps
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+int spm_tensor_map(spm_ctx *c, const void *ptr, int kind, CUtensorMap *out) {
+  for (size_t i = c->tmaps.size(); i-- > 0;)
+    if (c->tmaps[i].ptr == ptr && c->tmaps[i].kind == kind) {
+      *out = c->tmaps[i].map;
+      return SPM_OK;
+    }
+  if (((uintptr_t)ptr & 15u) != 0) return spm_fail(SPM_ERR_ARG, "spectrum buffers must be 16-byte aligned");
+  auto fn = encode_fn();
+  if (!fn) return spm_fail(SPM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const int N = c->N;
+  const size_t es = c->prec == SPM_FP64 ? 8 : 4;
+  const cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)N};  // N reals = N/2 complex per row
+  const cuuint64_t strides[2] = {(cuuint64_t)N * es, (cuuint64_t)N * N * es};
+  cuuint32_t box[3];
+  if (kind == TM_PENCIL) {
+    box[0] = 16;  // 8 complex columns
+    box[1] = 1;
+    box[2] = (cuuint32_t)N;
+  } else {
+    box[0] = 32;  // 16 complex columns
+    box[1] = (cuuint32_t)N;
+    box[2] = 1;
+  }
+  const cuuint32_t estr[3] = {1, 1, 1};
+  TmEntry e;
+  e.ptr = ptr;
+  e.kind = kind;
+  CUresult r = fn(&e.map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return spm_fail(SPM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  if (c->tmaps.size() >= 64) c->tmaps.erase(c->tmaps.begin());
+  c->tmaps.push_back(e);
+  *out = e.map;
+  return SPM_OK;
+}
+
+// Reads (and clears) the error word that bounded waits set on timeout.
+int spm_check_device_error(spm_ctx *c) {
+  int err = 0;
+  cudaError_t e = cudaMemcpy(&err, c->flow + FW_ERR, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "error word read");
+  if (err) {
+    cudaMemset(c->flow + FW_ERR, 0, sizeof(int));
+    return spm_fail(SPM_ERR_CUDA, "a kernel's bounded wait for its asynchronous copies timed out");
+  }
+  return SPM_OK;
+}
+
 int spm_read_scal(spm_ctx *c, int nb) {
   cudaError_t e = cudaMemcpyAsync(c->host_scal, c->scal, sizeof(double) * kScal * nb, cudaMemcpyDeviceToHost,
                                   c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "scalar read");
   e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "stream sync");
+  if (e != cudaSuccess) return spm_fail_cuda(e, "stream sync");
+  return spm_check_device_error(c);
 }
 
 extern "C" int spm_ctx_create(int N, double L, double Tau, double Gamma, double dt, int precision, void *stream,
@@ -160,12 +228,42 @@ extern "C" int spm_ctx_create(int N, double L, double Tau, double Gamma, double 
                    cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { spm_ctx_destroy(c); return spm_fail_cuda(e, "twiddles"); }
   }
+  // Spectral symbols per K^2 = Kx^2 + Ky^2 + Kz^2 (every K in [-N/2, N/2)):
+  // G(k^2) with k^2 = K^2 / L^2 (get_GK, Initialization.cpp:150-166), the
+  // gradient-step factor 1/(1 + dt G) (LPsrc.cpp:64-67), the preconditioner
+  // symbol 1/(G + |Tau| + 0.02) (Initialization.cpp:123-129) and the force-step
+  // factor 1/(1 + G) (SPM.cpp:82-86).
+  {
+    const int kmax = 3 * (N / 2) * (N / 2);
+    std::vector<double> tab(4 * (size_t)(kmax + 1));
+    const double ph = 0.568809, s2 = ph * ph, invL = 1.0 / L;
+    for (int K2 = 0; K2 <= kmax; K2++) {
+      const double k2 = (double)K2 * (invL * invL);
+      const double k4 = k2 * k2, k6 = k4 * k2, k8 = k6 * k2;
+      const double G = std::exp(-0.5 * k2 / s2) *
+                           (1.969182919080340 + -14.949858723012090 * k2 + 37.445683882581790 * k4 +
+                            -38.839451762550148 * k6 + 13.999261011773505 * k8) +
+                       0.08;
+      tab[4 * (size_t)K2 + 0] = G;
+      tab[4 * (size_t)K2 + 1] = 1.0 / (1.0 + dt * G);
+      tab[4 * (size_t)K2 + 2] = 1.0 / (G + std::fabs(Tau) + 0.02);
+      tab[4 * (size_t)K2 + 3] = 1.0 / (1.0 + G);
+    }
+    cudaError_t e = cudaMalloc(&c->gtab, sizeof(double) * tab.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(c->gtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      spm_ctx_destroy(c);
+      return spm_fail_cuda(e, "symbol table");
+    }
+  }
   cudaError_t e = cudaMalloc(&c->partials, sizeof(double) * kPartStride * kRedMax * kMaxBatch);
   if (e == cudaSuccess) e = cudaMalloc(&c->tickets, sizeof(unsigned) * kMaxBatch);
   if (e == cudaSuccess) e = cudaMemset(c->tickets, 0, sizeof(unsigned) * kMaxBatch);
   if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(double) * kScal * kMaxBatch);
   if (e == cudaSuccess) e = cudaMemset(c->scal, 0, sizeof(double) * kScal * kMaxBatch);
   if (e == cudaSuccess) e = cudaMalloc(&c->flow, sizeof(int) * 8);
+  if (e == cudaSuccess) e = cudaMemset(c->flow, 0, sizeof(int) * 8);
   if (e == cudaSuccess) e = cudaMallocHost(&c->host_scal, sizeof(double) * kScal * kMaxBatch);
   if (e == cudaSuccess) e = cudaMallocHost(&c->host_flow, sizeof(int) * 8);
   if (e != cudaSuccess) {
@@ -182,6 +280,7 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
   else cudaDeviceSynchronize();
   spm_free_extra(c);
   cudaFree(c->tw);
+  cudaFree(c->gtab);
   cudaFree(c->partials);
   cudaFree(c->tickets);
   cudaFree(c->scal);
@@ -197,6 +296,22 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
   return SPM_OK;
 }
 
+extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
+  if (!c || !knob) return spm_fail(SPM_ERR_ARG, "null argument");
+  if (std::strcmp(knob, "plane_cps") == 0) {
+    if (value != 1 && value != 2) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1 or 2");
+    c->plane_cps = value;
+    return SPM_OK;
+  }
+  return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
+}
+
+extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
+  if (!c || !knob) return -1;
+  if (std::strcmp(knob, "plane_cps") == 0) return c->plane_cps;
+  return -1;
+}
+
 extern "C" int spm_set_stream(spm_ctx *c, void *stream) {
   if (!c) return spm_fail(SPM_ERR_ARG, "ctx is NULL");
   c->stream = (cudaStream_t)stream;
@@ -206,7 +321,8 @@ extern "C" int spm_set_stream(spm_ctx *c, void *stream) {
 extern "C" int spm_sync(spm_ctx *c) {
   if (!c) return spm_fail(SPM_ERR_ARG, "ctx is NULL");
   cudaError_t e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "stream sync");
+  if (e != cudaSuccess) return spm_fail_cuda(e, "stream sync");
+  return spm_check_device_error(c);
 }
 
 extern "C" size_t spm_field_bytes(const spm_ctx *c) { return c ? c->field_bytes : 0; }
@@ -294,9 +410,10 @@ extern "C" int spm_grad_flow_enqueue(spm_ctx *c, void *phi, void *uhat, int nste
 
 extern "C" int spm_grad_flow_collect(spm_ctx *c, spm_step_stats *stats, int max_records, int *steps_done) {
   if (!c) return spm_fail(SPM_ERR_ARG, "ctx is NULL");
-  cudaError_t e = cudaMemcpyAsync(c->host_flow, c->flow, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = cudaMemcpyAsync(c->host_flow, c->flow, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "grad flow");
+  SPM_TRY(spm_check_device_error(c));
   const int done = c->host_flow[FW_ITER];
   if (steps_done) *steps_done = done;
   const int n = std::min(done, max_records);

@@ -2,10 +2,24 @@
 // libspmiqc_cuda.so (not part of the public ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fft_core.cuh"
+
+// Box shapes of the tensor copies over a packed spectrum [x][ky][2*(N/2) reals].
+enum TmKind {
+  TM_PENCIL = 0,    // 8 complex columns x 1 ky row x all N x
+  TM_PLANE_INV = 1  // 16 complex columns x all N ky x 1 x-plane
+};
+struct TmEntry {
+  const void *ptr;
+  int kind;
+  CUtensorMap map;
+};
 
 struct spm_ctx {
   int N = 0;
@@ -31,6 +45,9 @@ struct spm_ctx {
   void *host_phi = nullptr;     // device copies used by the host-buffer entry points
   void *host_uhat = nullptr;
   int *gate = nullptr;          // flow words gating every launch of a solver chain (or null)
+  double *gtab = nullptr;       // spectral symbols per K^2 (4 doubles each)
+  std::vector<TmEntry> tmaps;   // tensor-map cache (most recent last)
+  int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
 };
 
 int spm_fail(int status, const char *what);
@@ -40,5 +57,8 @@ int spm_ensure_scratch(spm_ctx *c, int nb);
 char *spm_bufA(spm_ctx *c, int b);
 char *spm_bufB(spm_ctx *c, int b);
 int spm_read_scal(spm_ctx *c, int nb);
+int spm_check_device_error(spm_ctx *c);
+// Tensor map of kind `kind` over the packed spectrum at ptr (cached per context).
+int spm_tensor_map(spm_ctx *c, const void *ptr, int kind, CUtensorMap *out);
 void spm_free_extra(spm_ctx *c);
 const struct OpsTable *spm_table_of(const spm_ctx *c);
