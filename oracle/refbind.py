@@ -15,10 +15,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libspmref.so")
+# the same harness with the hot-path routines resolved to the GPU compat layer
+COMPAT_LIB = os.path.join(HERE, "_ref", "libspmref_compat.so")
 REFDIR_DEFAULT = "/root/reference"
 
 _dp = ctypes.POINTER(ctypes.c_double)
-_lib = None
+_libs = {}
 
 
 def build(refdir: str = REFDIR_DEFAULT, quiet: bool = True) -> bool:
@@ -31,16 +33,25 @@ def build(refdir: str = REFDIR_DEFAULT, quiet: bool = True) -> bool:
     return True
 
 
-def available() -> bool:
-    return os.path.exists(LIB)
+def build_compat(refdir: str = REFDIR_DEFAULT) -> bool:
+    """Compile the drop-in check library (needs the CUDA library built)."""
+    if not os.path.isdir(os.path.join(refdir, "src")):
+        return os.path.exists(COMPAT_LIB)
+    out = subprocess.run(["make", "-C", HERE, f"REFDIR={refdir}", "compat"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("compat harness build failed:\n" + out.stdout + out.stderr)
+    return True
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(LIB)
-        L = ctypes.CDLL(LIB)
+def available(path: str = LIB) -> bool:
+    return os.path.exists(path)
+
+
+def lib(path: str = LIB):
+    if path not in _libs:
+        if not available(path):
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(path)
         L.ref_setup.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.ref_get_Ene.restype = ctypes.c_double
         L.ref_inpfp.restype = ctypes.c_double
@@ -50,8 +61,8 @@ def lib():
         L.ref_lobpcg_init.argtypes = [ctypes.c_int, ctypes.c_uint64, _dp]
         L.ref_lobpcg_inip.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp]
         L.ref_spring_pairing.argtypes = [_dp, _dp, ctypes.c_double, ctypes.c_double]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _p(a: np.ndarray):
@@ -62,9 +73,9 @@ def _p(a: np.ndarray):
 class Ref:
     """One configured reference instance (the reference keeps its state in globals)."""
 
-    def __init__(self, N, L=26.0, Tau=-0.0061, Gamma=0.30, dt=0.3, threads=1):
+    def __init__(self, N, L=26.0, Tau=-0.0061, Gamma=0.30, dt=0.3, threads=1, path=LIB):
         self.N, self.n3 = N, N ** 3
-        self.L = lib()
+        self.L = lib(path)
         self.L.ref_set_threads(int(threads))
         if self.L.ref_setup(N, L, Tau, Gamma, dt) != 0:
             raise ValueError("ref_setup failed")

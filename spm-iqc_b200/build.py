@@ -23,6 +23,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libspmiqc_cuda.so")
 COMPAT_LIB = os.path.join(LIBDIR, "libspmiqc_compat.so")
 
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
                   "-I", os.path.join(ROOT, "include")]
@@ -87,12 +88,16 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
             o = os.path.join(OBJ, "compat_" + os.path.basename(s) + ".o")
             cobjs.append(o)
             if force or _stale(o, [s] + headers):
-                cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c", s, "-o", o]
+                cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-I", os.path.join(ROOT, "include"),
+                       "-I", os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o]
                 out = subprocess.run(cmd, capture_output=True, text=True)
                 if out.returncode != 0:
                     raise RuntimeError("compat compile failed:\n" + out.stderr[-4000:])
         if force or _stale(COMPAT_LIB, cobjs + [LIB]):
+            # the reference's globals (N, u_R_local, ...) stay undefined here and
+            # resolve against the program that links the drop-in
             cmd = ["g++", "-shared", "-o", COMPAT_LIB] + cobjs + ["-L", LIBDIR, "-lspmiqc_cuda",
+                                                                   "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
                                                                    "-Wl,-rpath,$ORIGIN"]
             out = subprocess.run(cmd, capture_output=True, text=True)
             if out.returncode != 0:

@@ -31,6 +31,33 @@ def test_cuda_library_exports_every_declared_symbol():
     assert L.spm_supported_size(256) == 1 and L.spm_supported_size(100) == 0
 
 
+COMPAT_SIGNATURES = {
+    "my_fft(double (*) [2], double (*) [2])", "my_ifft(double (*) [2], double (*) [2])", "My_mpi_fft_set_up()",
+    "get_Ene()", "get_min_u_F()", "ngrad_cam(double (*) [2], double (*) [2])",
+    "hv_cam(double (*) [2], double (*) [2], double (*) [2])", "precond_camnew(double (*) [2])",
+    "hiosd_lobpcg_initialization(Option*, int)", "hiosd_lobpcg_inip(double (*) [2], Option*)",
+    "copy_option_V(Option*, Option*, int)", "copy_option_V(double (**) [2], Option*, int)",
+    "copy_option_V(double (*) [2], Option*, int)",
+    "get_Tv(double (**) [2], double (*) [2])", "Natural_Forces(double (*) [2], double (*) [2])",
+    "MinMax_Forces(double (*) [2], double (*) [2])", "Spring_Pairing(double (**) [2], double, double)",
+    "Gs_gri_nuc(double (*) [2], double (*) [2])",
+}
+
+
+def test_compat_library_exports_the_reference_signatures():
+    """Every C++ function of the reference's My_FFT / LPsrc / LOBPCG / SPM
+    objects is defined, with the same mangled name, by the drop-in."""
+    import shutil
+    import subprocess
+    lib = os.path.join(LIBDIR, "libspmiqc_compat.so")
+    if not os.path.exists(lib) or not shutil.which("nm"):
+        pytest.skip("compat library or nm missing")
+    out = subprocess.run(["nm", "-D", "-C", "--defined-only", lib], capture_output=True, text=True).stdout
+    have = {line.split(" ", 2)[2].strip() for line in out.splitlines() if " T " in line}
+    missing = COMPAT_SIGNATURES - have
+    assert not missing, missing
+
+
 def test_context_rejects_bad_arguments_without_gpu_work():
     lib = os.path.join(LIBDIR, "libspmiqc_cuda.so")
     if not os.path.exists(lib):
