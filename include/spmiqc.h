@@ -113,6 +113,25 @@ int spm_energy(spm_ctx *ctx, const void *phi, const void *uhat, double *energy);
 int spm_grad_flow(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol_grad,
                   spm_step_stats *stats, int *steps_done);
 
+/* Mixed-precision get_min_u_F (no counterpart in the reference): on an FP64
+ * context, runs the flow with FP32 transforms (FP64 reductions) until
+ * ||grad F|| <= switch_tol, then continues in FP64 from that state (phi cast
+ * to FP64, uhat = my_fft(phi)) until ||grad F|| <= tol_grad. stats (host, >=
+ * max_steps records, may be NULL) receives the FP32 steps then the FP64 ones. */
+int spm_grad_flow_mixed(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol_grad, double switch_tol,
+                        spm_step_stats *stats, int *steps_fp32, int *steps_fp64);
+
+/* Batched get_min_u_F over n independent instances (no counterpart in the
+ * reference; each context may have its own N, L, Tau, Gamma, dt): one
+ * captured CUDA graph advances every instance by steps_per_launch gated steps
+ * on parallel stream branches and is relaunched until all instances reached
+ * ||grad F|| <= tol_grad (or max_steps). With switch_tol > tol_grad the
+ * instances (FP64 contexts) first run with FP32 transforms to switch_tol,
+ * then in FP64. steps_done (host, n entries, may be NULL) receives the steps
+ * executed per instance. The contexts' streams are synchronised first. */
+int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n, int max_steps, double tol_grad,
+                        double switch_tol, int steps_per_launch, int *steps_done);
+
 /* The asynchronous form of spm_grad_flow: enqueues exactly nsteps gated steps
  * on the context stream and returns without synchronising (the stop rule is
  * evaluated on the device; steps after it do no work). Capturable in a CUDA

@@ -1,0 +1,175 @@
+// Batched gradient flows of independent instances (grids of any supported
+// sizes and parameters): one CUDA graph holds `steps_per_launch` gated steps of
+// every instance, each instance on its own stream branch, so one graph launch
+// advances all of them and small grids overlap on the device. Instances stop
+// on the device (convergence or their step cap); the graph is relaunched until
+// every instance has stopped. With switch_tol > 0 the instances first run on
+// their FP32 twins (FP32 transforms, FP64 reductions) to switch_tol, then on
+// FP64 to tol_grad.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/spmiqc.h"
+#include "blas1.cuh"
+#include "spm_internal.h"
+#include "spm_table.h"
+
+using namespace spm;
+
+#define SPM_TRY(x)               \
+  do {                           \
+    int _s = (x);                \
+    if (_s != SPM_OK) return _s; \
+  } while (0)
+
+namespace {
+
+struct Streams {
+  std::vector<cudaStream_t> s;
+  std::vector<cudaEvent_t> ev;
+  ~Streams() {
+    for (auto x : s) cudaStreamDestroy(x);
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+// Runs the flows of n contexts to tol (or max_steps each); steps[i] += done.
+int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int max_steps, double tol, int K,
+              int *steps) {
+  Streams st;
+  st.s.resize(n + 1);
+  st.ev.resize(n + 1);
+  for (int i = 0; i <= n; i++) {
+    if (cudaStreamCreateWithFlags(&st.s[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&st.ev[i], cudaEventDisableTiming) != cudaSuccess)
+      return spm_fail(SPM_ERR_CUDA, "batch streams");
+  }
+  cudaStream_t s0 = st.s[n];
+  std::vector<cudaStream_t> saved(n);
+  for (int i = 0; i < n; i++) {
+    saved[i] = ctx[i]->stream;
+    cudaStreamSynchronize(saved[i]);  // earlier work of the instance is complete
+    SPM_TRY(spm_ensure_scratch(ctx[i], 1));
+    SPM_TRY(spm_ensure_stats(ctx[i], max_steps + K));
+    SPM_TRY(spm_flow_init(ctx[i], s0));
+    ctx[i]->m.tol_grad = tol;
+    ctx[i]->m.max_steps = max_steps;
+  }
+  // one step of every instance outside the capture sets up kernel attributes
+  // and tensor maps; it counts as the first step of the flow
+  for (int i = 0; i < n; i++) {
+    ctx[i]->stream = s0;
+    SPM_TRY(spm_table_of(ctx[i])->grad_step(ctx[i], phi[i], uh[i]));
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "graph capture");
+  e = cudaEventRecord(st.ev[n], s0);
+  int rc = SPM_OK;
+  for (int i = 0; i < n && rc == SPM_OK && e == cudaSuccess; i++) {
+    e = cudaStreamWaitEvent(st.s[i], st.ev[n], 0);
+    ctx[i]->stream = st.s[i];
+    const OpsTable *t = spm_table_of(ctx[i]);
+    for (int k = 0; k < K && rc == SPM_OK; k++) rc = t->grad_step(ctx[i], phi[i], uh[i]);
+    if (e == cudaSuccess) e = cudaEventRecord(st.ev[i], st.s[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, st.ev[i], 0);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(s0, &graph);
+  if (rc != SPM_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return spm_fail_cuda(e, "graph instantiate");
+  }
+  std::vector<int> host(8 * (size_t)n);
+  const int launches = (max_steps + K - 1) / K;
+  for (int l = 0; l < launches && rc == SPM_OK; l++) {
+    e = cudaGraphLaunch(exec, s0);
+    if (e != cudaSuccess) {
+      rc = spm_fail_cuda(e, "graph launch");
+      break;
+    }
+    for (int i = 0; i < n; i++)
+      cudaMemcpyAsync(&host[8 * (size_t)i], ctx[i]->flow, sizeof(int) * 8, cudaMemcpyDeviceToHost, s0);
+    e = cudaStreamSynchronize(s0);
+    if (e != cudaSuccess) {
+      rc = spm_fail_cuda(e, "batch run");
+      break;
+    }
+    bool all = true;
+    for (int i = 0; i < n; i++) {
+      if (host[8 * (size_t)i + FW_ERR]) rc = spm_fail(SPM_ERR_CUDA, "a bounded wait timed out in a batched flow");
+      all = all && host[8 * (size_t)i + FW_GO] == 0;
+    }
+    if (all) break;
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  for (int i = 0; i < n; i++) {
+    ctx[i]->stream = saved[i];
+    ctx[i]->m.tol_grad = 0.0;
+    ctx[i]->m.max_steps = 0.0;
+    steps[i] += host[8 * (size_t)i + FW_ITER];
+  }
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n, int max_steps, double tol_grad,
+                                   double switch_tol, int steps_per_launch, int *steps_done) {
+  if (!ctx || !phi || !uhat || n < 1 || max_steps < 1 || steps_per_launch < 1 || !(tol_grad > 0))
+    return spm_fail(SPM_ERR_ARG, "bad argument");
+  for (int i = 0; i < n; i++)
+    if (!ctx[i] || !phi[i] || !uhat[i]) return spm_fail(SPM_ERR_ARG, "null instance");
+  std::vector<int> steps(n, 0);
+  if (switch_tol > tol_grad) {
+    for (int i = 0; i < n; i++)
+      if (ctx[i]->prec != SPM_FP64) return spm_fail(SPM_ERR_ARG, "mixed batches run on FP64 contexts");
+    std::vector<spm_ctx *> tw(n);
+    std::vector<void *> p32(n), u32(n);
+    for (int i = 0; i < n; i++) {
+      spm_ctx *c = ctx[i];
+      const size_t m = (size_t)c->N * c->N * c->N;
+      if (!c->twin) {
+        SPM_TRY(spm_ctx_create(c->N, c->L, c->m.Tau, c->m.Gamma, c->m.dt, SPM_FP32, c->stream, &c->twin));
+        c->twin->plane_cps = c->plane_cps;
+        cudaError_t e = cudaMalloc(&c->twin_buf, 2 * m * sizeof(float));
+        if (e != cudaSuccess) return spm_fail_cuda(e, "FP32 twin fields");
+      }
+      c->twin->stream = c->stream;
+      tw[i] = c->twin;
+      p32[i] = c->twin_buf;
+      u32[i] = (float *)c->twin_buf + m;
+      cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)phi[i], (float *)p32[i], m);
+      cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)uhat[i], (float *)u32[i], m);
+      c->launches += 2;
+    }
+    SPM_TRY(run_phase(tw.data(), p32.data(), u32.data(), n, max_steps, switch_tol, steps_per_launch,
+                      steps.data()));
+    for (int i = 0; i < n; i++) {
+      spm_ctx *c = ctx[i];
+      const size_t m = (size_t)c->N * c->N * c->N;
+      cast_kernel<float, double><<<1184, 256, 0, c->stream>>>((const float *)p32[i], (double *)phi[i], m);
+      c->launches++;
+      SPM_TRY(spm_fft(c, phi[i], uhat[i]));
+    }
+  }
+  int left = max_steps;
+  for (int i = 0; i < n; i++) left = std::min(left, max_steps - steps[i]);
+  if (left > 0)
+    SPM_TRY(run_phase(ctx, phi, uhat, n, left, tol_grad, steps_per_launch, steps.data()));
+  for (int i = 0; i < n; i++) {
+    cudaError_t e = cudaStreamSynchronize(ctx[i]->stream);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "batch");
+    if (steps_done) steps_done[i] = steps[i];
+  }
+  return SPM_OK;
+}

@@ -55,6 +55,13 @@ template <class T> struct ProSum {
   }
 };
 
+// Precision change of a real field or packed spectrum (n scalars).
+template <class Ti, class To>
+__global__ void cast_kernel(const Ti *__restrict__ in, To *__restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (To)in[i];
+}
+
 // Packed spectrum -> the reference's full complex spectrum (double, interleaved).
 template <class T>
 __global__ void packed_to_full_kernel(const c2<T> *__restrict__ pk, double2 *__restrict__ full, int N) {

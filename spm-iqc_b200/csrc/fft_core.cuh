@@ -327,6 +327,7 @@ struct ModelC {
   double ikt0;     // 1/(G0 + |Tau| + 0.02)
   double tol_grad; // grad-flow stop threshold on ||grad F|| (<= 0: off)
   double factor;   // SPM projection factor: 1 natural force, 2 min-max
+  double max_steps;  // grad-flow step cap evaluated on the device (<= 0: off)
 };
 
 // Grad-flow control words in device memory.

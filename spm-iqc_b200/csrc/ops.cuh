@@ -206,7 +206,9 @@ template <class T> struct OpGrad {
         p.stats[4 * it + 3] = tot[0];
       }
       p.flow[FW_ITER] = it + 1;
-      if (!(tot[1] > 1e-16) || (p.m.tol_grad > 0 && gn <= p.m.tol_grad)) p.flow[FW_PENDING] = 1;
+      if (!(tot[1] > 1e-16) || (p.m.tol_grad > 0 && gn <= p.m.tol_grad) ||
+          (p.m.max_steps > 0 && it + 1 >= p.m.max_steps))
+        p.flow[FW_PENDING] = 1;
     }
   }
 };

@@ -197,6 +197,7 @@ extern "C" int spm_ctx_create(int N, double L, double Tau, double Gamma, double 
   c->m.Tau = Tau;
   c->m.Gamma = Gamma;
   c->m.dt = dt;
+  c->L = L;
   c->m.invL = 1.0 / L;
   c->m.inv_n3 = 1.0 / n3;
   c->m.n3 = n3;
@@ -279,6 +280,8 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
   spm_free_extra(c);
+  if (c->twin) spm_ctx_destroy(c->twin);
+  cudaFree(c->twin_buf);
   cudaFree(c->tw);
   cudaFree(c->gtab);
   cudaFree(c->partials);
@@ -381,7 +384,17 @@ static __global__ void flow_init_kernel(int *flow) {
   flow[3] = 0;
 }
 
-static int ensure_stats(spm_ctx *c, int n) {
+int spm_flow_init(spm_ctx *c, cudaStream_t s) {
+  c->launches++;
+  flow_init_kernel<<<1, 1, 0, s>>>(c->flow);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "flow init");
+}
+
+int spm_ensure_stats(spm_ctx *c, int n);
+static int ensure_stats(spm_ctx *c, int n) { return spm_ensure_stats(c, n); }
+
+int spm_ensure_stats(spm_ctx *c, int n) {
   if (c->stats_cap >= n) return SPM_OK;
   if (c->stats) cudaStreamSynchronize(c->stream);
   cudaFree(c->stats);
@@ -454,6 +467,46 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
   c->m.tol_grad = 0.0;
   if (rc != SPM_OK) return rc;
   return spm_grad_flow_collect(c, stats, max_steps, steps_done);
+}
+
+// Mixed precision: FP32 transforms with FP64 reductions until ||grad F|| <=
+// switch_tol, then an FP64 polish from the FP32 state (phi in FP64, uhat =
+// my_fft(phi) recomputed in FP64) to tol_grad.
+extern "C" int spm_grad_flow_mixed(spm_ctx *c, void *phi, void *uhat, int max_steps, double tol_grad,
+                                   double switch_tol, spm_step_stats *stats, int *steps_fp32, int *steps_fp64) {
+  if (!c || !phi || !uhat || max_steps < 0 || !(tol_grad > 0)) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (c->prec != SPM_FP64) return spm_fail(SPM_ERR_ARG, "mixed precision runs on an FP64 context");
+  if (steps_fp32) *steps_fp32 = 0;
+  if (steps_fp64) *steps_fp64 = 0;
+  const size_t n = (size_t)c->N * c->N * c->N;
+  if (!c->twin) {
+    SPM_TRY(spm_ctx_create(c->N, c->L, c->m.Tau, c->m.Gamma, c->m.dt, SPM_FP32, c->stream, &c->twin));
+    c->twin->plane_cps = c->plane_cps;
+    cudaError_t e = cudaMalloc(&c->twin_buf, 2 * n * sizeof(float));
+    if (e != cudaSuccess) return spm_fail_cuda(e, "FP32 twin fields");
+  }
+  c->twin->stream = c->stream;
+  float *phi32 = (float *)c->twin_buf, *uh32 = phi32 + n;
+  c->launches += 2;
+  cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)phi, phi32, n);
+  cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)uhat, uh32, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
+  int n32 = 0, n64 = 0;
+  const double sw = switch_tol > tol_grad ? switch_tol : tol_grad;
+  SPM_TRY(spm_grad_flow(c->twin, phi32, uh32, max_steps, sw, stats, &n32));
+  c->launches += c->twin->launches;
+  c->twin->launches = 0;
+  c->launches++;
+  cast_kernel<float, double><<<1184, 256, 0, c->stream>>>(phi32, (double *)phi, n);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
+  SPM_TRY(spm_fft(c, phi, uhat));
+  const int left = max_steps - n32;
+  if (left > 0) SPM_TRY(spm_grad_flow(c, phi, uhat, left, tol_grad, stats ? stats + n32 : nullptr, &n64));
+  if (steps_fp32) *steps_fp32 = n32;
+  if (steps_fp64) *steps_fp64 = n64;
+  return SPM_OK;
 }
 
 extern "C" int spm_grad_flow_host(spm_ctx *c, void *phi_host, int max_steps, double tol_grad,

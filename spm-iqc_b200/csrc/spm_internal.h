@@ -27,6 +27,7 @@ struct spm_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   spm::ModelC m{};
+  double L = 0;             // box length as given
   size_t field_bytes = 0;   // bytes of one real field = bytes of one packed spectrum
   void *tw = nullptr;       // twiddle table exp(-2 pi i j/N) in the context precision
   double *partials = nullptr;
@@ -48,6 +49,8 @@ struct spm_ctx {
   double *gtab = nullptr;       // spectral symbols per K^2 (4 doubles each)
   std::vector<TmEntry> tmaps;   // tensor-map cache (most recent last)
   int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
+  spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
+  void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
 };
 
 int spm_fail(int status, const char *what);
@@ -58,6 +61,8 @@ char *spm_bufA(spm_ctx *c, int b);
 char *spm_bufB(spm_ctx *c, int b);
 int spm_read_scal(spm_ctx *c, int nb);
 int spm_check_device_error(spm_ctx *c);
+int spm_flow_init(spm_ctx *c, cudaStream_t s);    // go = 1, iter = 0
+int spm_ensure_stats(spm_ctx *c, int n);          // per-step record capacity
 // Tensor map of kind `kind` over the packed spectrum at ptr (cached per context).
 int spm_tensor_map(spm_ctx *c, const void *ptr, int kind, CUtensorMap *out);
 void spm_free_extra(spm_ctx *c);

@@ -177,6 +177,24 @@ class SpmContext:
                                   ctypes.byref(n)))
         return np.array([[s.energy, s.res, s.grad_norm, s.e1] for s in st[:n.value]]).reshape(-1, 4)
 
+    def get_min_u_F_mixed(self, phi, uhat, max_steps: int, tol_grad: float, switch_tol: float = 1e-6):
+        """FP32 flow to switch_tol, then FP64 polish to tol_grad (FP64 context).
+        Returns (stats (n, 4), steps_fp32, steps_fp64)."""
+        st = (StepStats * max(1, max_steps))()
+        a, b = ctypes.c_int(), ctypes.c_int()
+        f = lib().spm_grad_flow_mixed
+        f.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.POINTER(StepStats),
+                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        check(f(self.h, _ptr(phi), _ptr(uhat), int(max_steps), float(tol_grad), float(switch_tol), st,
+                ctypes.byref(a), ctypes.byref(b)))
+        n = a.value + b.value
+        return np.array([[s.energy, s.res, s.grad_norm, s.e1] for s in st[:n]]).reshape(-1, 4), a.value, b.value
+
+    def tune(self, knob: str, value: int):
+        f = lib().spm_tune
+        f.argtypes = [_vp, ctypes.c_char_p, ctypes.c_int]
+        check(f(self.h, knob.encode(), int(value)))
+
     def ngrad_cam(self, phi, grad=None):
         grad = self.field() if grad is None else grad
         nrm = ctypes.c_double()
