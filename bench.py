@@ -168,6 +168,72 @@ def reference_arm(args, rank, world):
     return 0
 
 
+SERVE_CAPS = {"relax": 4000, "lobpcg": 21, "spm": 300}
+
+
+def _serve_run(specs, fields, precision_of, slots, tol):
+    """Replays the arrival stream into a job server; returns per-job results and server stats."""
+    import spmiqc
+    srv = spmiqc.JobServer(max_slots=slots)
+    ids = []
+    t0 = time.perf_counter()
+    for s, (p0, p1) in zip(specs, fields):
+        delay = s.t_arrival - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        prec = precision_of(s.kind)
+        d = spmiqc.job_desc(s.kind, s.N, prec, k=4, max_steps=SERVE_CAPS[s.kind], L=s.L, Tau=s.Tau, tol=tol,
+                            switch_tol=1e-6 if prec == "mixed" else 0.0, seed=s.seed)
+        ids.append(srv.submit(d, p0, p1))
+    res = [srv.wait(i, field=False)[0] for i in ids]
+    st = srv.stats()
+    srv.close()
+    return res, st
+
+
+def serve_bench(args):
+    """Serving workload: a seeded Poisson stream (mean 4 jobs/s) of 70%
+    relaxations (FP32 + FP64 polish), 20% k=4 LOBPCG (FP64) and 10% SPM saddle
+    searches (FP32 + FP64 polish), N in {64, 128, 192, 256}, run through the
+    job server with concurrent slots, next to the same stream executed serially
+    in FP64 (one job at a time, as the reference's one-job-per-program
+    drivers do)."""
+    import numpy as np
+    import torch
+    import workloads
+    torch.cuda.set_device(0)
+    specs = workloads.serving_stream(seed=2024, n_jobs=args.serve_jobs, rate=4.0)
+    fields = []
+    for s in specs:
+        p = workloads.field(s, device="cuda")
+        fields.append(workloads.replicas(s, p) if s.kind == "spm" else (p, None))
+    torch.cuda.empty_cache()
+    tol = 1e-8
+    out = {}
+    for name, slots, prec in (("served", args.serve_slots, lambda k: "fp64" if k == "lobpcg" else "mixed"),
+                              ("serial_fp64", 1, lambda k: "fp64")):
+        res, st = _serve_run(specs, fields, prec, slots, tol)
+        ok = [r for r in res if r.status == 0]
+        span = max(r.t_end for r in res) - min(r.t_submit for r in res)
+        lat = np.array([r.t_end - r.t_submit for r in ok])
+        conv = {k: int(sum(1 for s, r in zip(specs, res) if s.kind == k and r.status == 0 and r.residual <= tol))
+                for k in SERVE_CAPS}
+        out[name] = {"jobs_per_s": len(ok) / span, "p50_s": float(np.percentile(lat, 50, method="inverted_cdf")),
+                     "p99_s": float(np.percentile(lat, 99, method="inverted_cdf")), "completed": len(ok),
+                     "failed": int(st.failed), "peak_running": int(st.peak_running),
+                     "peak_reserved_gb": st.peak_bytes / 1e9, "makespan_s": span, "reached_tol": conv}
+    kinds = {k: sum(1 for s in specs if s.kind == k) for k in SERVE_CAPS}
+    sizes = {str(n): sum(1 for s in specs if s.N == n) for n in (64, 128, 192, 256)}
+    line = {"metric": "serving jobs/s (Poisson 4/s, 70% relax / 20% LOBPCG k=4 / 10% SPM)",
+            "value": out["served"]["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True,
+            "p50_s": out["served"]["p50_s"], "p99_s": out["served"]["p99_s"], "served": out["served"],
+            "serial_fp64": out["serial_fp64"], "data": "synthetic",
+            "config": {"workload": "serving stream", "jobs": len(specs), "kinds": kinds, "sizes": sizes,
+                       "caps": SERVE_CAPS, "tol": tol, "slots": args.serve_slots, "seed": 2024}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,8 +243,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--only-flow", action="store_true",
                     help="run only the warm-up and timed gradient steps (used for ncu captures)")
+    ap.add_argument("--serve", action="store_true", help="run the serving workload instead (one JSON line)")
+    ap.add_argument("--serve-jobs", type=int, default=40)
+    ap.add_argument("--serve-slots", type=int, default=6)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.serve:
+        return serve_bench(args)
     rank, world, local = dist_setup()
     if args.impl == "reference":
         rc = reference_arm(args, rank, world)

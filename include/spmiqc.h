@@ -48,10 +48,13 @@ enum spm_status {
   SPM_ERR_NOMEM = 3,        /* device allocation refused */
   SPM_ERR_NONFINITE = 4,    /* a reduction returned NaN/Inf */
   SPM_ERR_UNSUPPORTED = 5,  /* grid size or precision not built */
-  SPM_ERR_STATE = 6         /* call order (e.g. LOBPCG block not initialised) */
+  SPM_ERR_STATE = 6,        /* call order (e.g. LOBPCG block not initialised) */
+  SPM_ERR_CANCELLED = 7     /* a job was cancelled (job server) */
 };
 
-enum spm_precision { SPM_FP64 = 0, SPM_FP32 = 1 };
+/* Contexts take SPM_FP64 or SPM_FP32; SPM_MIXED is a job precision of the job
+ * server (FP32 transforms to a switch tolerance, then an FP64 polish). */
+enum spm_precision { SPM_FP64 = 0, SPM_FP32 = 1, SPM_MIXED = 2 };
 
 /* Per-step record of a gradient-flow run (LPsrc.cpp:52-110). */
 typedef struct spm_step_stats {
@@ -195,6 +198,13 @@ int spm_minmax_forces(spm_ctx *ctx, void *x, const void *v);
  * iteration; *iters the iterations done. */
 int spm_spring_pairing(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double *res_hist,
                        int *iters);
+/* Mixed-precision Spring_Pairing (no counterpart in the reference): on an
+ * FP64 context, the natural-force and min-max steps run with FP32 transforms
+ * (FP64 reductions) until res <= switch_tol, then continue in FP64 from the
+ * cast replicas until res <= tol. res_hist (host, >= maxiter entries, may be
+ * NULL) receives the FP32 iterations' residuals, then the FP64 ones. */
+int spm_spring_pairing_mixed(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double switch_tol,
+                             double *res_hist, int *iters_fp32, int *iters_fp64);
 
 /* ------------------------------------------------------------ BLAS-1 */
 
@@ -215,6 +225,86 @@ int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
  * array's address; make it before any stream capture begins. */
 int spm_inpfp_batch_noalloc(size_t n, int nb, int precision, const void *p, const void *q,
                             double *out, void *stream);
+
+/* ------------------------------------------------------------ job server */
+
+/* A job server (no counterpart in the reference, whose drivers run one job
+ * per process: main_SPM.cpp, grad.cpp): relaxation, eigenmode and saddle
+ * jobs of any supported grid sizes share one GPU. Submitted jobs wait in
+ * arrival order; the oldest waiting job whose device-memory footprint fits in
+ * the free part of the budget and for which a slot is free starts at once, on
+ * its own stream and context, while the others run (smaller jobs may pass a
+ * large one that does not fit yet). Reductions are deterministic, so a job's
+ * result is the same alone and among others. */
+typedef struct spm_server spm_server;
+
+enum spm_job_kind {
+  SPM_JOB_RELAX = 0,  /* get_min_u_F to ||grad F|| <= tol (max_steps cap) */
+  SPM_JOB_LOBPCG = 1, /* hiosd_lobpcg_initialization(seed) + inip at phi0, k modes */
+  SPM_JOB_SPM = 2     /* Spring_Pairing of the replicas (phi0, phi1) to res <= tol */
+};
+
+typedef struct spm_job_desc {
+  int kind;        /* spm_job_kind */
+  int N;           /* grid size (spm_supported_size) */
+  int precision;   /* SPM_FP64, SPM_FP32 or SPM_MIXED (relaxation and SPM) */
+  int k;           /* LOBPCG block size, 1..8 */
+  int max_steps;   /* step / iteration cap */
+  int reserved;
+  double L, Tau, Gamma, dt;
+  double tol;        /* ||grad F|| (relaxation), residual (LOBPCG, SPM) */
+  double switch_tol; /* SPM_MIXED: FP32 until this tolerance (0: 1e-6) */
+  uint64_t seed;     /* LOBPCG start block */
+} spm_job_desc;
+
+typedef struct spm_job_result {
+  int status;        /* SPM_OK, SPM_ERR_CANCELLED, SPM_ERR_NOMEM, ... */
+  int steps;         /* steps / iterations executed */
+  double energy;     /* relaxation: final energy; SPM: energy of phi1 */
+  double residual;   /* final ||grad F||, max LOBPCG residual or SPM res */
+  double evals[8];   /* LOBPCG eigenvalues */
+  double t_submit, t_start, t_end; /* seconds since the server was created */
+} spm_job_result;
+
+typedef struct spm_server_config {
+  size_t budget_bytes;  /* device bytes jobs may hold at once (0: 90% of free) */
+  int max_slots;        /* jobs running at once */
+  int fake_device;      /* nonzero: no GPU work; a job sleeps fake_ms_per_munit
+                           ms per million grid points per step */
+  double fake_ms_per_munit;
+  size_t fake_device_bytes; /* fake device memory; an allocation beyond it is
+                               refused (0: unlimited) */
+  int max_bypass;       /* times later jobs may start before a waiting job
+                           that does not fit (0: 8) */
+} spm_server_config;
+
+typedef struct spm_server_stats {
+  int64_t completed, failed, cancelled, pending;
+  int running, peak_running;
+  size_t peak_bytes, budget_bytes;
+  double p50_s, p99_s;  /* submit-to-end latency of completed jobs */
+  double elapsed_s;     /* since the server was created */
+} spm_server_stats;
+
+int spm_server_create(const spm_server_config *cfg, spm_server **out);
+/* Device bytes the server reserves for a job while it runs. */
+size_t spm_job_footprint(const spm_job_desc *job);
+/* phi0 (and phi1 for SPM_JOB_SPM) are host arrays of N^3 doubles, copied at
+ * submission. A job larger than the whole budget is refused (SPM_ERR_NOMEM). */
+int spm_server_submit(spm_server *srv, const spm_job_desc *job, const double *phi0, const double *phi1,
+                      int64_t *job_id);
+/* Cancels a waiting job, or asks a running one to stop at its next host
+ * check (between chunks of steps); its status becomes SPM_ERR_CANCELLED. */
+int spm_server_cancel(spm_server *srv, int64_t job_id);
+/* Waits for a job (block != 0) or polls it (SPM_ERR_STATE while unfinished).
+ * field (may be NULL) receives the result as doubles: the relaxed phi (N^3),
+ * the k eigenvectors (k N^3) or the replica phi1 (N^3). */
+int spm_server_wait(spm_server *srv, int64_t job_id, int block, spm_job_result *result, double *field);
+/* Drops the record of a finished job (its result field and times). */
+int spm_server_release(spm_server *srv, int64_t job_id);
+int spm_server_get_stats(spm_server *srv, spm_server_stats *stats);
+/* Waits for every submitted job, then releases the server. */
+int spm_server_destroy(spm_server *srv);
 
 #ifdef __cplusplus
 }

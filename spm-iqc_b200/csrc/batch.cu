@@ -138,13 +138,7 @@ extern "C" int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n
     for (int i = 0; i < n; i++) {
       spm_ctx *c = ctx[i];
       const size_t m = (size_t)c->N * c->N * c->N;
-      if (!c->twin) {
-        SPM_TRY(spm_ctx_create(c->N, c->L, c->m.Tau, c->m.Gamma, c->m.dt, SPM_FP32, c->stream, &c->twin));
-        c->twin->plane_cps = c->plane_cps;
-        cudaError_t e = cudaMalloc(&c->twin_buf, 2 * m * sizeof(float));
-        if (e != cudaSuccess) return spm_fail_cuda(e, "FP32 twin fields");
-      }
-      c->twin->stream = c->stream;
+      SPM_TRY(spm_ensure_twin(c));
       tw[i] = c->twin;
       p32[i] = c->twin_buf;
       u32[i] = (float *)c->twin_buf + m;

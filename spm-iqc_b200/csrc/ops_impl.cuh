@@ -3,6 +3,8 @@
 // through the OpsTable of the context.
 #pragma once
 
+#include <atomic>
+
 #include "blas1.cuh"
 #include "spm_internal.h"
 #include "spm_table.h"
@@ -18,10 +20,12 @@ namespace spm {
 // Sets the dynamic shared-memory limit of a kernel once per device. Tag makes
 // the "done" bits distinct per kernel (the kernels share one function type).
 template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, int dev) {
-  static unsigned done = 0;  // one bit per device (first 32)
-  if (dev < 32 && (done >> dev) & 1u) return cudaSuccess;
+  // one bit per device (first 32); contexts on several host threads may race
+  // here, which at worst sets the attribute twice
+  static std::atomic<unsigned> done{0};
+  if (dev < 32 && (done.load(std::memory_order_acquire) >> dev) & 1u) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess && dev < 32) done |= 1u << dev;
+  if (e == cudaSuccess && dev < 32) done.fetch_or(1u << dev, std::memory_order_release);
   return e;
 }
 
@@ -42,16 +46,20 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  static int ncl[32] = {0};
+  // the grid depends only on the kernel and the device (never on the load),
+  // so the reductions' partial sums, and hence the results, do not either
+  static std::atomic<int> ncl[32] = {};
   const int dev = c->device < 32 ? c->device : 0;
-  if (ncl[dev] == 0) {
+  int nc = ncl[dev].load(std::memory_order_relaxed);
+  if (nc == 0) {
     cfg.gridDim = dim3(Geo<N>::CL * N, 1, 1);
     int n = 0;
     e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
     if (e != cudaSuccess || n < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, what);
-    ncl[dev] = n < N ? n : N;
+    nc = n < N ? n : N;
+    ncl[dev].store(nc, std::memory_order_relaxed);
   }
-  cfg.gridDim = dim3(Geo<N>::CL * ncl[dev], nb, 1);
+  cfg.gridDim = dim3(Geo<N>::CL * nc, nb, 1);
   c->launches++;
   e = cudaLaunchKernelEx(&cfg, kern, p);
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, what);
@@ -89,18 +97,20 @@ template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams 
   struct Tag {};
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, "pencil attribute");
-  static int nblk[32] = {0};
+  static std::atomic<int> nblk[32] = {};
   const int dev = c->device < 32 ? c->device : 0;
-  if (nblk[dev] == 0) {
+  int nbk = nblk[dev].load(std::memory_order_relaxed);
+  if (nbk == 0) {
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     if (e != cudaSuccess || per_sm < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration,
                                                              "pencil occupancy");
-    nblk[dev] = per_sm * sms < Geo<N>::PTILES ? per_sm * sms : Geo<N>::PTILES;
+    nbk = per_sm * sms < Geo<N>::PTILES ? per_sm * sms : Geo<N>::PTILES;
+    nblk[dev].store(nbk, std::memory_order_relaxed);
   }
   c->launches++;
-  kern<<<dim3(nblk[dev], nb, 1), kThreads, smem, c->stream>>>(p);
+  kern<<<dim3(nbk, nb, 1), kThreads, smem, c->stream>>>(p);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, "pencil launch");
 }

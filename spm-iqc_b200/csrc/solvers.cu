@@ -393,6 +393,7 @@ extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxit
       rmax = std::max(rmax, res[i]);
     }
     if (it >= maxiter || (tol > 0 && rmax <= tol)) break;
+    if (spm_cancelled(c)) return spm_fail(SPM_ERR_CANCELLED, "cancelled");
     // W = P0(precond(W)), W perp V, W Gram-Schmidt with dropping (LOBPCG.cpp:287-308)
     SPM_TRY(precond_many(c, W.data(), k));
     SPM_TRY(project_out(c, Vc.data(), k, W.data(), k));
@@ -559,6 +560,10 @@ extern "C" int spm_spring_pairing(spm_ctx *c, void *phi0, void *phi1, int maxite
       break;
     }
     if (c->host_flow[FW_GO] == 0) break;
+    if (spm_cancelled(c)) {
+      rc = spm_fail(SPM_ERR_CANCELLED, "cancelled");
+      break;
+    }
     chunk = std::min(chunk * 2, 64);
   }
   c->gate = nullptr;
@@ -571,5 +576,38 @@ extern "C" int spm_spring_pairing(spm_ctx *c, void *phi0, void *phi1, int maxite
     for (int i = 0; i < done; i++)
       if (!std::isfinite(res_hist[i])) return spm_fail(SPM_ERR_NONFINITE, "non-finite SPM residual");
   }
+  return SPM_OK;
+}
+
+// Mixed precision: the replica pair runs on the FP32 twin (FP32 transforms,
+// FP64 reductions) until res <= switch_tol, then in FP64 from the cast
+// replicas until res <= tol.
+extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int maxiter, double tol,
+                                        double switch_tol, double *res_hist, int *iters_fp32, int *iters_fp64) {
+  if (!c || !phi0 || !phi1 || maxiter < 0 || !(tol > 0)) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (c->prec != SPM_FP64) return spm_fail(SPM_ERR_ARG, "mixed precision runs on an FP64 context");
+  if (iters_fp32) *iters_fp32 = 0;
+  if (iters_fp64) *iters_fp64 = 0;
+  const size_t n = npts(c);
+  SPM_TRY(spm_ensure_twin(c));
+  float *a = (float *)c->twin_buf, *b = a + n;
+  c->launches += 2;
+  cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)phi0, a, n);
+  cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)phi1, b, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
+  int n32 = 0, n64 = 0;
+  const double sw = switch_tol > tol ? switch_tol : tol;
+  SPM_TRY(spm_spring_pairing(c->twin, a, b, maxiter, sw, res_hist, &n32));
+  c->launches += c->twin->launches + 2;
+  c->twin->launches = 0;
+  cast_kernel<float, double><<<1184, 256, 0, c->stream>>>(a, (double *)phi0, n);
+  cast_kernel<float, double><<<1184, 256, 0, c->stream>>>(b, (double *)phi1, n);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
+  const int left = maxiter - n32;
+  if (left > 0) SPM_TRY(spm_spring_pairing(c, phi0, phi1, left, tol, res_hist ? res_hist + n32 : nullptr, &n64));
+  if (iters_fp32) *iters_fp32 = n32;
+  if (iters_fp64) *iters_fp64 = n64;
   return SPM_OK;
 }

@@ -40,6 +40,7 @@ extern "C" const char *spm_status_str(int s) {
     case SPM_ERR_NONFINITE: return "non-finite result";
     case SPM_ERR_UNSUPPORTED: return "unsupported size or precision";
     case SPM_ERR_STATE: return "invalid call order";
+    case SPM_ERR_CANCELLED: return "cancelled";
     default: return "unknown status";
   }
 }
@@ -462,11 +463,25 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { rc = spm_fail_cuda(e, "grad flow"); break; }
     if (c->host_flow[FW_GO] == 0) break;
+    if (spm_cancelled(c)) { rc = spm_fail(SPM_ERR_CANCELLED, "cancelled"); break; }
     chunk = std::min(chunk * 2, 256);
   }
   c->m.tol_grad = 0.0;
   if (rc != SPM_OK) return rc;
   return spm_grad_flow_collect(c, stats, max_steps, steps_done);
+}
+
+int spm_ensure_twin(spm_ctx *c) {
+  if (!c->twin) {
+    const size_t n = (size_t)c->N * c->N * c->N;
+    SPM_TRY(spm_ctx_create(c->N, c->L, c->m.Tau, c->m.Gamma, c->m.dt, SPM_FP32, c->stream, &c->twin));
+    cudaError_t e = cudaMalloc(&c->twin_buf, 2 * n * sizeof(float));
+    if (e != cudaSuccess) return spm_fail_cuda(e, "FP32 twin fields");
+  }
+  c->twin->stream = c->stream;
+  c->twin->cancel = c->cancel;
+  c->twin->plane_cps = c->plane_cps;
+  return SPM_OK;
 }
 
 // Mixed precision: FP32 transforms with FP64 reductions until ||grad F|| <=
@@ -479,13 +494,7 @@ extern "C" int spm_grad_flow_mixed(spm_ctx *c, void *phi, void *uhat, int max_st
   if (steps_fp32) *steps_fp32 = 0;
   if (steps_fp64) *steps_fp64 = 0;
   const size_t n = (size_t)c->N * c->N * c->N;
-  if (!c->twin) {
-    SPM_TRY(spm_ctx_create(c->N, c->L, c->m.Tau, c->m.Gamma, c->m.dt, SPM_FP32, c->stream, &c->twin));
-    c->twin->plane_cps = c->plane_cps;
-    cudaError_t e = cudaMalloc(&c->twin_buf, 2 * n * sizeof(float));
-    if (e != cudaSuccess) return spm_fail_cuda(e, "FP32 twin fields");
-  }
-  c->twin->stream = c->stream;
+  SPM_TRY(spm_ensure_twin(c));
   float *phi32 = (float *)c->twin_buf, *uh32 = phi32 + n;
   c->launches += 2;
   cast_kernel<double, float><<<1184, 256, 0, c->stream>>>((const double *)phi, phi32, n);

@@ -51,7 +51,10 @@ struct spm_ctx {
   int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
+  const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)
 };
+
+inline bool spm_cancelled(const spm_ctx *c) { return c->cancel && *c->cancel; }
 
 int spm_fail(int status, const char *what);
 int spm_fail_cuda(cudaError_t e, const char *what);
@@ -66,4 +69,7 @@ int spm_ensure_stats(spm_ctx *c, int n);          // per-step record capacity
 // Tensor map of kind `kind` over the packed spectrum at ptr (cached per context).
 int spm_tensor_map(spm_ctx *c, const void *ptr, int kind, CUtensorMap *out);
 void spm_free_extra(spm_ctx *c);
+// Creates (once) the FP32 twin context and its two FP32 fields, and binds it
+// to the context's stream, cancel flag and tuning.
+int spm_ensure_twin(spm_ctx *c);
 const struct OpsTable *spm_table_of(const spm_ctx *c);

@@ -19,7 +19,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libspmiqc_cuda.so")
 
-SPM_FP64, SPM_FP32 = 0, 1
+SPM_FP64, SPM_FP32, SPM_MIXED = 0, 1, 2
+SPM_JOB_RELAX, SPM_JOB_LOBPCG, SPM_JOB_SPM = 0, 1, 2
+SPM_ERR_NOMEM, SPM_ERR_STATE, SPM_ERR_CANCELLED = 3, 6, 7
 _vp = ctypes.c_void_p
 _lib = None
 
@@ -33,6 +35,32 @@ class SpmError(RuntimeError):
 class StepStats(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("res", ctypes.c_double),
                 ("grad_norm", ctypes.c_double), ("e1", ctypes.c_double)]
+
+
+class JobDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("N", ctypes.c_int), ("precision", ctypes.c_int), ("k", ctypes.c_int),
+                ("max_steps", ctypes.c_int), ("reserved", ctypes.c_int), ("L", ctypes.c_double),
+                ("Tau", ctypes.c_double), ("Gamma", ctypes.c_double), ("dt", ctypes.c_double),
+                ("tol", ctypes.c_double), ("switch_tol", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("steps", ctypes.c_int), ("energy", ctypes.c_double),
+                ("residual", ctypes.c_double), ("evals", ctypes.c_double * 8), ("t_submit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_end", ctypes.c_double)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("fake_device", ctypes.c_int),
+                ("fake_ms_per_munit", ctypes.c_double), ("fake_device_bytes", ctypes.c_size_t),
+                ("max_bypass", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("cancelled", ctypes.c_int64),
+                ("pending", ctypes.c_int64), ("running", ctypes.c_int), ("peak_running", ctypes.c_int),
+                ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("p50_s", ctypes.c_double),
+                ("p99_s", ctypes.c_double), ("elapsed_s", ctypes.c_double)]
 
 
 def lib():
@@ -69,6 +97,16 @@ def lib():
             "spm_minmax_forces": [_vp, _vp, _vp],
             "spm_spring_pairing": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_int)],
+            "spm_spring_pairing_mixed": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)],
+            "spm_server_create": [ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)],
+            "spm_server_submit": [_vp, ctypes.POINTER(JobDesc), _vp, _vp, ctypes.POINTER(ctypes.c_int64)],
+            "spm_server_cancel": [_vp, ctypes.c_int64],
+            "spm_server_wait": [_vp, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(JobResult), _vp],
+            "spm_server_release": [_vp, ctypes.c_int64],
+            "spm_server_get_stats": [_vp, ctypes.POINTER(ServerStats)],
+            "spm_server_destroy": [_vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -79,6 +117,8 @@ def lib():
         L.spm_status_str.argtypes = [ctypes.c_int]
         L.spm_field_bytes.restype = ctypes.c_size_t
         L.spm_field_bytes.argtypes = [_vp]
+        L.spm_job_footprint.restype = ctypes.c_size_t
+        L.spm_job_footprint.argtypes = [ctypes.POINTER(JobDesc)]
         L.spm_launch_count.restype = ctypes.c_uint64
         L.spm_launch_count.argtypes = [_vp]
         _lib = L
@@ -253,6 +293,14 @@ class SpmContext:
                                        ctypes.byref(it)))
         return np.array(hist[:it.value])
 
+    def Spring_Pairing_mixed(self, phi0, phi1, maxiter: int, tol: float, switch_tol: float = 1e-6):
+        """FP32 iterations to switch_tol, then FP64 to tol; returns (history, fp32 iterations, fp64 iterations)."""
+        hist = (ctypes.c_double * max(1, maxiter))()
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(lib().spm_spring_pairing_mixed(self.h, _ptr(phi0), _ptr(phi1), int(maxiter), float(tol),
+                                             float(switch_tol), hist, ctypes.byref(a), ctypes.byref(b)))
+        return np.array(hist[:a.value + b.value]), a.value, b.value
+
     # ---- BasicOperators.cpp
     def inpfp(self, p, q) -> float:
         out = ctypes.c_double()
@@ -261,3 +309,93 @@ class SpmContext:
 
     def nrmp(self, p) -> float:
         return float(np.sqrt(self.inpfp(p, p)))
+
+
+_KINDS = {"relax": SPM_JOB_RELAX, "lobpcg": SPM_JOB_LOBPCG, "spm": SPM_JOB_SPM}
+_PRECS = {"fp64": SPM_FP64, "fp32": SPM_FP32, "mixed": SPM_MIXED}
+
+
+def job_desc(kind: str, N: int, precision: str = "fp64", k: int = 4, max_steps: int = 1000, L: float = 26.0,
+             Tau: float = -0.0061, Gamma: float = 0.30, dt: float = 0.3, tol: float = 1e-8,
+             switch_tol: float = 0.0, seed: int = 0) -> JobDesc:
+    return JobDesc(_KINDS[kind], int(N), _PRECS[precision], int(k), int(max_steps), 0, float(L), float(Tau),
+                   float(Gamma), float(dt), float(tol), float(switch_tol), int(seed))
+
+
+def job_footprint(desc: JobDesc) -> int:
+    return int(lib().spm_job_footprint(ctypes.byref(desc)))
+
+
+class JobServer:
+    """The library's job server (spm_server_*): jobs of mixed kinds and grid
+    sizes admitted by device-memory footprint into max_slots concurrent slots.
+    fake_device=True runs the scheduler without a GPU (jobs sleep
+    fake_ms_per_munit ms per million grid points per step)."""
+
+    def __init__(self, budget_bytes: int = 0, max_slots: int = 4, fake_device: bool = False,
+                 fake_ms_per_munit: float = 0.0, fake_device_bytes: int = 0, max_bypass: int = 0):
+        if not fake_device:
+            import torch
+            if not torch.cuda.is_available():
+                raise RuntimeError("spmiqc needs a CUDA device (no CPU path)")
+        cfg = ServerConfig(int(budget_bytes), int(max_slots), int(bool(fake_device)), float(fake_ms_per_munit),
+                           int(fake_device_bytes), int(max_bypass))
+        h = _vp()
+        check(lib().spm_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.sizes = {}
+
+    def submit(self, desc: JobDesc, phi0: np.ndarray, phi1: np.ndarray | None = None) -> int:
+        p0 = np.ascontiguousarray(phi0, dtype=np.float64)
+        p1 = None if phi1 is None else np.ascontiguousarray(phi1, dtype=np.float64)
+        jid = ctypes.c_int64()
+        check(lib().spm_server_submit(self.h, ctypes.byref(desc), p0.ctypes.data,
+                                      None if p1 is None else p1.ctypes.data, ctypes.byref(jid)))
+        n = desc.N ** 3
+        self.sizes[jid.value] = (desc.k * n if desc.kind == SPM_JOB_LOBPCG else n, desc.N)
+        return jid.value
+
+    def cancel(self, jid: int):
+        check(lib().spm_server_cancel(self.h, int(jid)))
+
+    def wait(self, jid: int, block: bool = True, field: bool = True):
+        """Returns (JobResult, field or None), or None if the job is unfinished (block=False)."""
+        res = JobResult()
+        cnt, N = self.sizes[jid]
+        out = np.empty(cnt, dtype=np.float64) if field else None
+        st = lib().spm_server_wait(self.h, int(jid), int(block), ctypes.byref(res),
+                                   None if out is None else out.ctypes.data)
+        if st == SPM_ERR_STATE and not block:
+            return None
+        check(st)
+        if out is not None and res.status == 0:
+            out = out.reshape((-1, N, N, N)) if cnt != N ** 3 else out.reshape((N, N, N))
+        elif out is not None:
+            out = None
+        return res, out
+
+    def release(self, jid: int):
+        check(lib().spm_server_release(self.h, int(jid)))
+        self.sizes.pop(jid, None)
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        check(lib().spm_server_get_stats(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spm_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
