@@ -264,6 +264,7 @@ typedef struct spm_job_result {
   double residual;   /* final ||grad F||, max LOBPCG residual or SPM res */
   double evals[8];   /* LOBPCG eigenvalues */
   double t_submit, t_start, t_end; /* seconds since the server was created */
+  char message[128];  /* spm_last_error() of a failed job, else empty */
 } spm_job_result;
 
 typedef struct spm_server_config {

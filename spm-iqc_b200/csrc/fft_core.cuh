@@ -363,6 +363,11 @@ __device__ __forceinline__ double4 symbols(const KParams &p, int Kx, int Ky, int
   return make_double4(a.x, a.y, c.x, c.y);
 }
 
+// Half `h` of the symbols at K^2 (h = 0: {G, 1/(1+dt G)}, h = 1: {1/(G+|Tau|+0.02), 1/(1+G)}).
+__device__ __forceinline__ double2 symbols_half(const KParams &p, int k2, int h) {
+  return __ldg(reinterpret_cast<const double2 *>(p.gtab) + 2 * k2 + h);
+}
+
 // Signed wave number of index i on an N grid (Initialization.cpp:97-107).
 __device__ __forceinline__ int wave(int i, int N) { return i < N / 2 ? i : i - N; }
 

@@ -45,9 +45,12 @@ template <int N, class T, int CPS> constexpr size_t plane_smem() {
   return sizeof(c2<T>) * (N + N / 2 + Geo<N>::PLANE_UNITS + (CPS == 1 ? Geo<N>::STAGE_UNITS : 0)) + 16 +
          sizeof(double) * 32 * kRedMax + 128;
 }
-template <int N, class T> constexpr size_t pencil_smem(int stages) {
+// Pencil symbol table (per tile): 9 kz rows (the tile's 8 columns and kz = N/2)
+// x |Kx| = 0..N/2, one double2 half of the K^2 symbols each.
+template <int N> constexpr int pencil_sym_entries() { return 9 * (N / 2 + 1); }
+template <int N, class T> constexpr size_t pencil_smem(int stages, bool sym) {
   return sizeof(c2<T>) * (N + Geo<N>::PENCIL_UNITS + (size_t)stages * Geo<N>::STAGE_UNITS) + 16 +
-         sizeof(double) * 32 * kRedMax + 128;
+         sizeof(double) * 32 * kRedMax + (sym ? sizeof(double2) * pencil_sym_entries<N>() : 0) + 128;
 }
 
 __device__ __forceinline__ unsigned char *smem_base128(unsigned char *raw) {
@@ -259,6 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
   T2 *sS = sA + (Op::FI ? G::STAGE_UNITS : 0);
   uint64_t *bars = reinterpret_cast<uint64_t *>(ex + G::PENCIL_UNITS + NST * G::STAGE_UNITS);
   double *red = reinterpret_cast<double *>(bars + 2);
+  double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbols of the current tile
   __shared__ int s_err;
   if (flow_stopped(p)) return;
 
@@ -270,6 +274,27 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
   // Tiles run columns-fastest, so concurrently resident CTAs read adjacent
   // 8-column segments of the same ky rows.
   constexpr int NCH = M / 8;
+  // Symbols: a tile's points have |Ky| = t (rows t and N - t, t > 0), Kz in
+  // its 8 columns (or N/2 for the packed c = 0 column) and any Kx, so the
+  // 9 x (N/2 + 1) entries it needs are staged in shared memory, fetched into
+  // registers one tile ahead (the table lookups of every point would
+  // otherwise wait on L2). Tiles with t = 0 (rows 0 and N/2) read the table.
+  constexpr bool USE_SYM = Op::SYM >= 0;
+  constexpr int KXS = N / 2 + 1, SYMN = pencil_sym_entries<N>();
+  constexpr int SPT = USE_SYM ? (SYMN + kThreads - 1) / kThreads : 1;
+  double2 pre[SPT];
+  auto sym_fetch = [&](int tl) {
+    const int tt = tl / NCH, cz = (tl % NCH) * 8;
+#pragma unroll
+    for (int i = 0; i < SPT; i++) {
+      const int e = tid + i * kThreads;
+      if (e < SYMN) {
+        const int row = e / KXS, a = e - row * KXS;
+        const int kz = row < 8 ? cz + row : N / 2;
+        pre[i] = symbols_half(p, a * a + tt * tt + kz * kz, USE_SYM ? Op::SYM : 0);
+      }
+    }
+  };
   // thread 0: two tensor boxes (8 columns x all x) for rows ky0, ky1 of a tile
   auto issue = [&](const CUtensorMap *map, T2 *dst, uint64_t *bar, int tile) {
     const int t = tile / NCH, c0 = (tile % NCH) * 8;
@@ -294,6 +319,8 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
     if (Op::FI) issue(&p.tmi[b], sA, &bars[0], tile);
     if (Op::SI) issue(&p.tms[b], sS, &bars[1], tile);
   }
+  if constexpr (USE_SYM)
+    if (tile < G::PTILES && tile / NCH != 0) sym_fetch(tile);
 
   for (int it = 0; tile < G::PTILES; tile += gridDim.x, it++) {
     const int next = tile + gridDim.x;
@@ -303,6 +330,25 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
     const int ky = rowsel ? ky1 : ky0;
     const int col = c0 + cc;
     const bool dc = (c0 == 0);
+    if constexpr (USE_SYM) {
+      // the previous tile's point operator is done (barrier at the loop end)
+      if (t != 0) {
+#pragma unroll
+        for (int i = 0; i < SPT; i++)
+          if (tid + i * kThreads < SYMN) stab[tid + i * kThreads] = pre[i];
+      }
+      if (next < G::PTILES && next / NCH != 0) sym_fetch(next);
+      if constexpr (!Op::FI) __syncthreads();
+    }
+    // symbols of (Kx, Ky, Kz) for kz row `row` of the tile (8: kz = N/2)
+    auto sym_at = [&](int Kx, int Ky, int Kz, int row) -> double2 {
+      if constexpr (!USE_SYM) {
+        return double2{0.0, 0.0};
+      } else {
+        if (t != 0) return stab[row * KXS + (Kx < 0 ? -Kx : Kx)];
+        return symbols_half(p, Kx * Kx + Ky * Ky + Kz * Kz, Op::SYM);
+      }
+    };
 
     T2 F[16];
     if constexpr (Op::FI) {
@@ -375,12 +421,12 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
             sM = T2{(T)0.5 * (s.y + q.y), (T)0.5 * (q.x - s.x)};
           }
           T2 so0, inv0, soM, invM;
-          Op::point(p, b, Kx, Ky, 0, f0, s0, so0, inv0, acc, 1.0);
-          Op::point(p, b, Kx, Ky, -N / 2, fM, sM, soM, invM, acc, 1.0);
+          Op::point(p, b, Kx, Ky, 0, sym_at(Kx, Ky, 0, 0), f0, s0, so0, inv0, acc, 1.0);
+          Op::point(p, b, Kx, Ky, -N / 2, sym_at(Kx, Ky, N / 2, 8), fM, sM, soM, invM, acc, 1.0);
           o_st = T2{so0.x - soM.y, so0.y + soM.x};
           o_inv = T2{inv0.x - invM.y, inv0.y + invM.x};
         } else {
-          Op::point(p, b, Kx, Ky, col, f, s, o_st, o_inv, acc, dc && cc == 0 ? 1.0 : 2.0);
+          Op::point(p, b, Kx, Ky, col, sym_at(Kx, Ky, col, cc), f, s, o_st, o_inv, acc, dc && cc == 0 ? 1.0 : 2.0);
         }
         if constexpr (Op::SO) so[((size_t)kx * N + ky) * M + col] = o_st;
         F[k2] = o_inv;

@@ -140,10 +140,11 @@ template <class T> struct ProTangent {
 // Forward transform with the reference's 1/N^3 (My_FFT.cpp:9-13): store only.
 template <class T> struct OpFwd {
   static constexpr bool FI = true, SI = false, SO = true, INV = false, LIN = true;
+  static constexpr int SYM = -1;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int, int, int, int, c2<T> f, c2<T>, c2<T> &so, c2<T> &,
-                               double (&)[1], double) {
+  __device__ static void point(const KParams &p, int, int, int, int, double2, c2<T> f, c2<T>, c2<T> &so,
+                               c2<T> &, double (&)[1], double) {
     so = cscale(f, (T)p.m.inv_n3);
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -152,9 +153,10 @@ template <class T> struct OpFwd {
 // Backward transform of a stored spectrum (My_FFT.cpp:15-21): inverse only.
 template <class T> struct OpInv {
   static constexpr bool FI = false, SI = true, SO = false, INV = true, LIN = true;
+  static constexpr int SYM = -1;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &, int, int, int, int, c2<T>, c2<T> s, c2<T> &, c2<T> &inv,
+  __device__ static void point(const KParams &, int, int, int, int, double2, c2<T>, c2<T> s, c2<T> &, c2<T> &inv,
                                double (&)[1], double) {
     inv = s;
   }
@@ -167,11 +169,11 @@ template <class T> struct OpInv {
 //   E1 = 1/2 sum G |u|^2,  ||grad F||^2 = sum_{k != 0} |G u - f^|^2.
 template <class T> struct OpGrad {
   static constexpr bool FI = true, SI = true, SO = true, INV = true, LIN = false;
+  static constexpr int SYM = 0;  // {G, 1/(1 + dt G)}
   static constexpr int NR = 3;
   static constexpr unsigned MAXM = 0x2;
-  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &so,
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T> s, c2<T> &so,
                                c2<T> &inv, double (&acc)[3], double w) {
-    const double4 sy = symbols(p, Kx, Ky, Kz);
     const double G = sy.x;
     const T dt = (T)p.m.dt;
     const c2<T> fh = cscale(f, (T)p.m.inv_n3);
@@ -217,11 +219,12 @@ template <class T> struct OpGrad {
 // mode is kept) or, with ZERO_DC, for ngrad_cam (LPsrc.cpp:133-142).
 template <class T, bool ZERO_DC> struct OpGmul {
   static constexpr bool FI = true, SI = false, SO = false, INV = true, LIN = false;
+  static constexpr int SYM = 0;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T>, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const T g = (T)symbols(p, Kx, Ky, Kz).x;
+    const T g = (T)sy.x;
     inv = cscale(cscale(f, (T)p.m.inv_n3), g);
     if (ZERO_DC && Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
   }
@@ -231,11 +234,12 @@ template <class T, bool ZERO_DC> struct OpGmul {
 // Preconditioner symbol 1/(G + |Tau| + 0.02) (Initialization.cpp:123-129, LOBPCG.cpp:175-179).
 template <class T> struct OpPrecond {
   static constexpr bool FI = true, SI = false, SO = false, INV = true, LIN = false;
+  static constexpr int SYM = 1;  // {1/(G + |Tau| + 0.02), 1/(1 + G)}
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &,
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T>, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const T ik = (T)symbols(p, Kx, Ky, Kz).z;  // 1 / (G + |Tau| + 0.02)
+    const T ik = (T)sy.x;  // 1 / (G + |Tau| + 0.02)
     inv = cscale(cscale(f, (T)p.m.inv_n3), ik);
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -246,11 +250,12 @@ template <class T> struct OpPrecond {
 // spectrum of the tangent.
 template <class T> struct OpForce {
   static constexpr bool FI = true, SI = true, SO = false, INV = true, LIN = false;
+  static constexpr int SYM = 1;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T> s, c2<T> &,
+  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T> s, c2<T> &,
                                c2<T> &inv, double (&)[1], double) {
-    const T iden = (T)symbols(p, Kx, Ky, Kz).w;  // 1 / (1 + G)
+    const T iden = (T)sy.y;  // 1 / (1 + G)
     const T sc = (T)scal_of(p, b)[SC_S];
     const c2<T> fh = cscale(f, (T)p.m.inv_n3);
     inv = c2<T>{(fh.x - sc * s.x) * iden, (fh.y - sc * s.y) * iden};
@@ -264,14 +269,15 @@ template <class T> struct OpForce {
 // field is taken as given (||d|| := 1), for force steps along a caller's v.
 template <class T, bool NORM = true> struct OpTangent {
   static constexpr bool FI = true, SI = false, SO = true, INV = true, LIN = false;
+  static constexpr int SYM = 0;
   static constexpr int NR = 0;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, c2<T> f, c2<T>, c2<T> &so,
+  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T>, c2<T> &so,
                                c2<T> &inv, double (&)[1], double) {
     const T inrm = NORM ? (T)(1.0 / sqrt(scal_of(p, b)[SC_NRM2])) : (T)1;
     const c2<T> v = cscale(cscale(f, (T)p.m.inv_n3), inrm);
     so = v;
-    const T g = (T)symbols(p, Kx, Ky, Kz).x;
+    const T g = (T)sy.x;
     inv = (Kx == 0 && Ky == 0 && Kz == 0) ? c2<T>{0, 0} : cscale(v, g);
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
@@ -280,11 +286,12 @@ template <class T, bool NORM = true> struct OpTangent {
 // E1 = 1/2 sum_k G |u_k|^2 of a stored spectrum (LPsrc.cpp:27-35): reduction only.
 template <class T> struct OpE1 {
   static constexpr bool FI = false, SI = true, SO = false, INV = false, LIN = false;
+  static constexpr int SYM = 0;
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
-  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, c2<T>, c2<T> s, c2<T> &, c2<T> &,
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T>, c2<T> s, c2<T> &, c2<T> &,
                                double (&acc)[1], double w) {
-    const double G = symbols(p, Kx, Ky, Kz).x;
+    const double G = sy.x;
     acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {

@@ -93,7 +93,7 @@ template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams 
     if (Op::SI) SPM_TRY(spm_tensor_map(c, p.st[b], TM_PENCIL, &p.tms[b]));
   }
   auto kern = pencil_kernel<N, T, Op>;
-  constexpr size_t smem = pencil_smem<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0));
+  constexpr size_t smem = pencil_smem<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0);
   struct Tag {};
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, "pencil attribute");

@@ -19,6 +19,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -262,6 +263,10 @@ void worker_loop(spm_server *S) {
     lk.unlock();
     int rc = S->cfg.fake_device ? run_job_fake(S, j) : run_job_gpu(S, j);
     if (rc != SPM_OK && j->cancel) rc = SPM_ERR_CANCELLED;
+    if (rc != SPM_OK) {
+      const char *m = rc == SPM_ERR_CANCELLED ? "cancelled" : spm_last_error();
+      std::snprintf(j->r.message, sizeof(j->r.message), "%s", m ? m : "");
+    }
     lk.lock();
     j->t_end = Clock::now();
     j->r.status = rc;
@@ -369,6 +374,7 @@ extern "C" int spm_server_cancel(spm_server *S, int64_t id) {
     j->state = JS_DONE;
     j->t_start = j->t_end = Clock::now();
     j->r.status = SPM_ERR_CANCELLED;
+    std::snprintf(j->r.message, sizeof(j->r.message), "cancelled before it started");
     j->r.t_submit = secs(S->t0, j->t_submit);
     j->r.t_start = j->r.t_end = secs(S->t0, j->t_end);
     S->cancelled++;

@@ -47,7 +47,7 @@ class JobDesc(ctypes.Structure):
 class JobResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("steps", ctypes.c_int), ("energy", ctypes.c_double),
                 ("residual", ctypes.c_double), ("evals", ctypes.c_double * 8), ("t_submit", ctypes.c_double),
-                ("t_start", ctypes.c_double), ("t_end", ctypes.c_double)]
+                ("t_start", ctypes.c_double), ("t_end", ctypes.c_double), ("message", ctypes.c_char * 128)]
 
 
 class ServerConfig(ctypes.Structure):

@@ -10,6 +10,11 @@ serving_stream(seed, n_jobs, rate): Poisson arrivals (mean `rate` jobs/s);
 70% relaxations, 20% k=4 LOBPCG eigenmode solves, 10% SPM saddle searches;
 N from {64, 128, 192, 256}; L ~ U[18, 30], Tau ~ U[-0.02, 0], amplitude
 ~ U[0.1, 0.2], N(0, 1e-3) noise.
+
+The amplitude is the rms of the cosine sum (each of the m cosines has
+amplitude amp * sqrt(2/m)), so fields over 8, 12 or 30 vectors have the same
+size. Taken per cosine instead, a 30-vector sum reaches |phi| ~ 3 and the
+explicit cubic term makes the semi-implicit step at dt = 0.3 diverge.
 """
 from __future__ import annotations
 
@@ -64,8 +69,9 @@ def field(spec: JobSpec, N: int | None = None, device: str | None = None) -> np.
     N = N or spec.N
     vec = shell_vectors(spec.shell, spec.L)
     vec = vec[np.all(np.abs(vec) < N // 2, axis=1)]
+    amp = spec.amp * np.sqrt(2.0 / len(vec))
     if device is None:
-        return inputs.cosine_shell(N, vec, amp=spec.amp, seed=spec.seed, noise=1e-3)
+        return inputs.cosine_shell(N, vec, amp=amp, seed=spec.seed, noise=1e-3)
     import torch
     theta = 2 * np.pi * inputs.unit(spec.seed, np.arange(len(vec), dtype=np.uint64))
     i = torch.arange(N, device=device, dtype=torch.float64) * (2 * np.pi / N)
@@ -73,7 +79,7 @@ def field(spec: JobSpec, N: int | None = None, device: str | None = None) -> np.
     for n, th in zip(vec, theta):
         phi += torch.cos(float(n[0]) * i[:, None, None] + float(n[1]) * i[None, :, None]
                          + float(n[2]) * i[None, None, :] + float(th))
-    phi *= spec.amp
+    phi *= amp
     g = torch.Generator(device=device)
     g.manual_seed(spec.seed)
     phi += 1e-3 * torch.randn((N, N, N), device=device, dtype=torch.float64, generator=g)
