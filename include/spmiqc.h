@@ -83,6 +83,9 @@ const char *spm_status_str(int status);
 /* Tuning knobs (no counterpart in the reference; the analogue of FFTW's plan
  * choice, My_FFT.cpp:49-97). knob "plane_cps": 1 = plane kernels stage their
  * input in shared memory (one CTA per SM), 2 = direct loads, two CTAs per SM.
+ * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
+ * inverse plane pass with the next step's forward one (phi stays on chip
+ * between steps; the same bits as 0), 0 = three passes per step.
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);

@@ -73,7 +73,7 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     e = cudaStreamWaitEvent(st.s[i], st.ev[n], 0);
     ctx[i]->stream = st.s[i];
     const OpsTable *t = spm_table_of(ctx[i]);
-    for (int k = 0; k < K && rc == SPM_OK; k++) rc = t->grad_step(ctx[i], phi[i], uh[i]);
+    rc = t->grad_steps(ctx[i], phi[i], uh[i], K);
     if (e == cudaSuccess) e = cudaEventRecord(st.ev[i], st.s[i]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, st.ev[i], 0);
   }

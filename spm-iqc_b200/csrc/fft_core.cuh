@@ -54,13 +54,22 @@ template <class T> using c2 = typename V2<T>::type;
 
 template <class T2> using base_t = decltype(T2::x);
 
+// Rounded product and fused multiply-add, never re-contracted by the
+// compiler. Sums of two products (complex products, rotations) are written
+// with them so every kernel rounds the same operation the same way: the
+// fused and the separate plane passes then produce identical bits.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
 template <class T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return {a.x + b.x, a.y + b.y}; }
 template <class T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) { return {a.x - b.x, a.y - b.y}; }
 template <class T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
-  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+  return {fma_rn(a.x, b.x, -mul_rn(a.y, b.y)), fma_rn(a.x, b.y, mul_rn(a.y, b.x))};
 }
 template <class T2> __device__ __forceinline__ T2 cmulc(T2 a, T2 b) {  // a * conj(b)
-  return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+  return {fma_rn(a.x, b.x, mul_rn(a.y, b.y)), fma_rn(a.y, b.x, -mul_rn(a.x, b.y))};
 }
 template <class T2> __device__ __forceinline__ T2 cconj(T2 a) { return {a.x, -a.y}; }
 template <class T2, class S> __device__ __forceinline__ T2 cscale(T2 a, S s) {
@@ -97,7 +106,7 @@ template <int DIR, int P, int E, class T2> __device__ __forceinline__ T2 twc(T2 
     using T = base_t<T2>;
     constexpr T c = (T)kTw240[e * (240 / P)][0];
     constexpr T s = (T)(DIR * kTw240[e * (240 / P)][1]);
-    return {v.x * c - v.y * s, v.x * s + v.y * c};
+    return {fma_rn(v.x, c, -mul_rn(v.y, s)), fma_rn(v.x, s, mul_rn(v.y, c))};
   }
 }
 
@@ -121,8 +130,8 @@ template <int DIR, class T2> struct Dft<DIR, 3, T2> {
     constexpr T h = (T)0.8660254037844386467637232;  // sqrt(3)/2
     T2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
     T2 x0 = cadd(v[0], t1);
-    T2 m = {v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
-    T2 n = mul_di<DIR>(cscale(t2, h));
+    T2 m = {fma_rn((T)-0.5, t1.x, v[0].x), fma_rn((T)-0.5, t1.y, v[0].y)};
+    T2 n = mul_di<DIR>(T2{mul_rn(t2.x, h), mul_rn(t2.y, h)});
     v[0] = x0;
     v[1] = cadd(m, n);
     v[2] = csub(m, n);
@@ -146,10 +155,10 @@ template <int DIR, class T2> struct Dft<DIR, 5, T2> {
     T2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
     T2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
     T2 x0 = cadd(v[0], cadd(t1, t2));
-    T2 b1 = {v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y};
-    T2 b2 = {v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y};
-    T2 d1 = mul_di<DIR>(T2{s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y});
-    T2 d2 = mul_di<DIR>(T2{s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y});
+    T2 b1 = {fma_rn(c2, t2.x, fma_rn(c1, t1.x, v[0].x)), fma_rn(c2, t2.y, fma_rn(c1, t1.y, v[0].y))};
+    T2 b2 = {fma_rn(c1, t2.x, fma_rn(c2, t1.x, v[0].x)), fma_rn(c1, t2.y, fma_rn(c2, t1.y, v[0].y))};
+    T2 d1 = mul_di<DIR>(T2{fma_rn(s1, t3.x, mul_rn(s2, t4.x)), fma_rn(s1, t3.y, mul_rn(s2, t4.y))});
+    T2 d2 = mul_di<DIR>(T2{fma_rn(s2, t3.x, -mul_rn(s1, t4.x)), fma_rn(s2, t3.y, -mul_rn(s1, t4.y))});
     v[0] = x0;
     v[1] = cadd(b1, d1);
     v[4] = csub(b1, d1);

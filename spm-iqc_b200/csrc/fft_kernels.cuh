@@ -65,83 +65,32 @@ __device__ __forceinline__ void report_error(const KParams &p, int s_err) {
   if (s_err && p.err && threadIdx.x == 0) atomicExch(p.err, 1);
 }
 
-// --------------------------------------------------------------- plane_fwd
-// Pro: static constexpr int NR; static constexpr unsigned MAXM;
-//      __device__ static T2 pro(const KParams&, int b, size_t idx, T2 x, double (&acc)[NR]);
-//        (x = reals idx, idx+1 of the input field; returns the values to transform)
-//      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
-// CPS = CTAs per SM the variant is built for: 1 stages the next plane's rows
-// in shared memory with a bulk copy; 2 has no stage (half the shared memory,
-// so two CTAs share an SM) and loads its rows straight from global memory.
-template <int N, class T, class Pro, int CPS>
-__global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
+// --------------------------------------------------------------- plane phases
+// The line-transform phases of the plane passes, shared by plane_fwd,
+// plane_inv and the fused plane_inv_fwd. A CTA of a cluster owns kRows = 32
+// z-rows (real space) and kCols = 16 packed spectral columns of the current
+// x-plane; `buf` is its exchange area, which the other CTAs of the cluster
+// read through distributed shared memory.
+template <int N, class T> struct Plane {
   using G = Geo<N>;
   using T2 = c2<T>;
-  constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
-  constexpr bool STAGED = (CPS == 1);
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
-  T2 *ztw = tw + N;                  // ztw[k1*8 + j2] = w^{2 j2 k1}
-  T2 *buf = ztw + N / 2;
-  T2 *stage = buf + G::PLANE_UNITS;  // 32 rows of N reals
-  uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
-  double *red = reinterpret_cast<double *>(bar + 2);
-  __shared__ int s_err;
-  if (flow_stopped(p)) return;
+  static constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
 
-  cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int b = blockIdx.y;
-  const int rank = (int)cluster.block_rank();
-  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
-  const T *src = reinterpret_cast<const T *>(p.in[b]);
-  auto issue = [&](int plane) {  // warp 0: one bulk copy per row of this CTA
-    if (lane == 0) mbar_expect_tx(bar, (unsigned)(kRows * N * sizeof(T)));
-    __syncwarp();
-    bulk_g2s(stage + lane * (N / 2), src + ((size_t)plane * N + rank * kRows + lane) * N, N * sizeof(T), bar);
-  };
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    s_err = 0;
-    fence_barrier_init();
+  // forward z, stage 1 of task (row r, j2): v = row elements j = j1*8 + j2
+  // (after the prologue); radix-N1 DFT, twiddle, store into the z exchange.
+  __device__ static void zf1_store(T2 *buf, const T2 *ztw, T2 (&v)[N1], int r, int j2) {
+    Dft<-1, N1, T2>::run(v);
+    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
+    sfor<0, N1>([&](auto K1) {
+      constexpr int k1 = SPM_CI(K1);
+      E[k1] = (k1 == 0) ? v[k1] : cmul(v[k1], ztw[k1 * 8 + j2]);
+    });
   }
-  for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
-  __syncthreads();
-  for (int i = tid; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
-  double acc[Pro::NR > 0 ? Pro::NR : 1];
-#pragma unroll
-  for (int r = 0; r < (Pro::NR > 0 ? Pro::NR : 1); r++) acc[r] = ((Pro::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
-  int plane = cid;
-  if (STAGED && warp == 0 && plane < N) issue(plane);
-  __syncthreads();
 
-  for (int it = 0; plane < N; plane += ncl, it++) {
-    const int next = plane + ncl;
-    if (STAGED) mbar_wait(bar, it & 1, &s_err);
-    // ---- z, stage 1: task (row r, j2), 8 threads per row; element j = j1*8 + j2
-    {
-      const int j2 = tid & 7, r = tid >> 3;
-      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
-      const T2 *row = STAGED ? stage + r * (N / 2) : reinterpret_cast<const T2 *>(src + rowoff);
-      T2 v[N1];
-      sfor<0, N1>([&](auto J1) {
-        constexpr int j1 = SPM_CI(J1);
-        const int j = j1 * 8 + j2;
-        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : __ldg(row + j), acc);
-      });
-      Dft<-1, N1, T2>::run(v);
-      T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
-      sfor<0, N1>([&](auto K1) {
-        constexpr int k1 = SPM_CI(K1);
-        E[k1] = (k1 == 0) ? v[k1] : cmul(v[k1], ztw[k1 * 8 + j2]);
-      });
-    }
-    __syncthreads();
-    if (STAGED && warp == 0 && next < N) {
-      fence_proxy_async();
-      issue(next);
-    }
-    // ---- z, stage 2: task (r, k1), 8-point DFT over j2 -> k = k1 + N1*k2
+  // forward z, stage 2 (8-point DFTs over j2 -> k = k1 + N1*k2) and the
+  // real-to-complex post-processing of the packed lines (pairs q, M-q). Ends
+  // with a cluster barrier: the rows [r][M] are then ready for remote reads.
+  __device__ static void zf2_post(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster) {
     {
       constexpr int NT = kRows * N1;
       constexpr int TPT = (NT + kThreads - 1) / kThreads;
@@ -168,7 +117,6 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       }
     }
     __syncthreads();
-    // ---- z, real-to-complex post-processing of the packed line (pairs k, M-k)
     {
       constexpr int NT = kRows * (M / 2);
       for (int task = tid; task < NT; task += kThreads) {
@@ -193,7 +141,13 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       }
     }
     cluster.sync();
-    // ---- y, stage 1: task (column c, j2); element y = 16*j1 + j2 lives in CTA y/32
+  }
+
+  // forward y over this CTA's 16 columns: gather element y = 16*j1 + j2 of
+  // column c from the CTA holding row y, radix-M1 DFT, exchange, radix-16
+  // DFT, store the spectral column into dst[plane][ky][M].
+  __device__ static void yf(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster, T2 *dst,
+                            int plane) {
     {
       const int c = tid & 15, j2 = tid >> 4;
       const int col = rank * kCols + c;
@@ -212,7 +166,6 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       });
     }
     __syncthreads();
-    // ---- y, stage 2: task (c, k1) -> ky = k1 + M1*k2; write the spectral column
     if (tid < 16 * M1) {
       const int c = tid & 15, k1 = tid >> 4;
       const int col = rank * kCols + c;
@@ -220,13 +173,242 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
 #pragma unroll
       for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
       Dft<-1, 16, T2>::run(u);
-      T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
 #pragma unroll
       for (int k2 = 0; k2 < 16; k2++) {
         const int ky = k1 + M1 * k2;
         dst[((size_t)plane * N + ky) * M + col] = u[k2];
       }
     }
+  }
+
+  // inverse y over this CTA's 16 columns; ld(ky, c) returns the input value.
+  // Leaves [y][16 columns] in buf and ends with a cluster barrier.
+  template <class LD>
+  __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld) {
+    {
+      const int c = tid & 15, j2 = tid >> 4;
+      T2 v[M1];
+      sfor<0, M1>([&](auto J1) {
+        constexpr int j1 = SPM_CI(J1);
+        v[j1] = ld(16 * j1 + j2, c);
+      });
+      Dft<+1, M1, T2>::run(v);
+      sfor<0, M1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
+      });
+    }
+    __syncthreads();
+    {
+      T2 u[16];
+      const int c = tid & 15, k1 = tid >> 4;
+      if (tid < 16 * M1) {
+#pragma unroll
+        for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+        Dft<+1, 16, T2>::run(u);
+      }
+      __syncthreads();
+      if (tid < 16 * M1) {
+#pragma unroll
+        for (int k2 = 0; k2 < 16; k2++) buf[(k1 + M1 * k2) * 16 + c] = u[k2];
+      }
+    }
+    cluster.sync();
+  }
+
+  // complex-to-real pre-processing: gather the pairs (q, M-q) of this CTA's
+  // rows from the column owners, then store the rows [r][M].
+  __device__ static void c2r_pre(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster) {
+    constexpr int NT = kRows * (M / 2);
+    constexpr int TPT = NT / kThreads;  // N/32 tasks per thread
+    static_assert(NT % kThreads == 0, "task count");
+    T2 za[TPT], zb[TPT];
+#pragma unroll
+    for (int i = 0; i < TPT; i++) {
+      const int task = tid + i * kThreads;
+      const int r = task / (M / 2), q = task % (M / 2);
+      const int y = rank * kRows + r;
+      if (q == 0) {
+        const T2 *r0 = cluster.map_shared_rank(buf, 0u);
+        const T2 *rh = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols));
+        const T2 P = r0[y * 16 + 0];
+        const T2 a = rh[y * 16 + (M / 2) % kCols];
+        // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
+        za[i] = T2{P.x + P.y, P.x - P.y};
+        // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
+        const T2 e = {a.x + a.x, (T)0};
+        const T2 o = {(T)0, a.y + a.y};
+        zb[i] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
+      } else {
+        const T2 *ra = cluster.map_shared_rank(buf, (unsigned)(q / kCols));
+        const T2 *rb = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols));
+        const T2 a = ra[y * 16 + q % kCols];
+        const T2 c = rb[y * 16 + (M - q) % kCols];
+        // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
+        const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
+        const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
+        za[i] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
+        zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
+      }
+    }
+    cluster.sync();
+#pragma unroll
+    for (int i = 0; i < TPT; i++) {
+      const int task = tid + i * kThreads;
+      const int r = task / (M / 2), q = task % (M / 2);
+      T2 *Z = buf + r * M;
+      if (q == 0) {
+        Z[0] = za[i];
+        Z[M / 2] = zb[i];
+      } else {
+        Z[q] = za[i];
+        Z[M - q] = zb[i];
+      }
+    }
+    __syncthreads();
+  }
+
+  // inverse z, stage 1 of task (r, j2): rows [r][M] -> z exchange.
+  __device__ static void zi1(T2 *buf, const T2 *ztw, int tid) {
+    const int j2 = tid & 7, r = tid >> 3;
+    T2 v[N1];
+    sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
+    __syncthreads();
+    Dft<+1, N1, T2>::run(v);
+    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
+    sfor<0, N1>([&](auto K1) {
+      constexpr int k1 = SPM_CI(K1);
+      E[k1] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
+    });
+    __syncthreads();
+  }
+
+  // inverse z, stage 2 of task (r, k1): 8-point DFTs; sink(r, j, z_j) gets
+  // z_j = y_{2j} + i y_{2j+1}, j = k1 + N1*k2. With TO_SMEM the sink may
+  // overwrite buf: every task is read first, then a barrier, then the sinks.
+  template <bool TO_SMEM, class SINK> __device__ static void zi2(T2 *buf, int tid, SINK sink) {
+    constexpr int NT = kRows * N1;
+    constexpr int TPT = (NT + kThreads - 1) / kThreads;
+    if constexpr (!TO_SMEM) {
+#pragma unroll
+      for (int t2 = 0; t2 < TPT; t2++) {
+        const int task = tid + t2 * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
+          T2 u[8];
+#pragma unroll
+          for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          Dft<+1, 8, T2>::run(u);
+#pragma unroll
+          for (int k2 = 0; k2 < 8; k2++) sink(r, k1 + N1 * k2, u[k2]);
+        }
+      }
+    } else {
+      T2 u[TPT][8];
+#pragma unroll
+      for (int t2 = 0; t2 < TPT; t2++) {
+        const int task = tid + t2 * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
+#pragma unroll
+          for (int j2 = 0; j2 < 8; j2++) u[t2][j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          Dft<+1, 8, T2>::run(u[t2]);
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int t2 = 0; t2 < TPT; t2++) {
+        const int task = tid + t2 * kThreads;
+        if (task < NT) {
+          const int r = task / N1, k1 = task % N1;
+#pragma unroll
+          for (int k2 = 0; k2 < 8; k2++) sink(r, k1 + N1 * k2, u[t2][k2]);
+        }
+      }
+    }
+  }
+};
+
+// Loads the twiddles into shared memory: tw[j] = exp(-2 pi i j/N) and the
+// z-stage table ztw[k1*8 + j2] = w^{2 j2 k1}.
+template <int N, class T> __device__ __forceinline__ void plane_twiddles(const KParams &p, c2<T> *tw, c2<T> *ztw) {
+  for (int i = threadIdx.x; i < N; i += kThreads) tw[i] = reinterpret_cast<const c2<T> *>(p.tw)[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
+}
+
+// --------------------------------------------------------------- plane_fwd
+// Pro: static constexpr int NR; static constexpr unsigned MAXM;
+//      __device__ static T2 pro(const KParams&, int b, size_t idx, T2 x, double (&acc)[NR]);
+//        (x = reals idx, idx+1 of the input field; returns the values to transform)
+//      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
+// CPS = CTAs per SM the variant is built for: 1 stages the next plane's rows
+// in shared memory with a bulk copy; 2 has no stage (half the shared memory,
+// so two CTAs share an SM) and loads its rows straight from global memory.
+template <int N, class T, class Pro, int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
+  using G = Geo<N>;
+  using T2 = c2<T>;
+  using P = Plane<N, T>;
+  constexpr int N1 = G::N1;
+  constexpr bool STAGED = (CPS == 1);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
+  T2 *ztw = tw + N;                  // ztw[k1*8 + j2] = w^{2 j2 k1}
+  T2 *buf = ztw + N / 2;
+  T2 *stage = buf + G::PLANE_UNITS;  // 32 rows of N reals
+  uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
+  double *red = reinterpret_cast<double *>(bar + 2);
+  __shared__ int s_err;
+  if (flow_stopped(p)) return;
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.y;
+  const int rank = (int)cluster.block_rank();
+  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  const T *src = reinterpret_cast<const T *>(p.in[b]);
+  T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
+  auto issue = [&](int plane) {  // warp 0: one bulk copy per row of this CTA
+    if (lane == 0) mbar_expect_tx(bar, (unsigned)(kRows * N * sizeof(T)));
+    __syncwarp();
+    bulk_g2s(stage + lane * (N / 2), src + ((size_t)plane * N + rank * kRows + lane) * N, N * sizeof(T), bar);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    s_err = 0;
+    fence_barrier_init();
+  }
+  plane_twiddles<N, T>(p, tw, ztw);
+  double acc[Pro::NR > 0 ? Pro::NR : 1];
+#pragma unroll
+  for (int r = 0; r < (Pro::NR > 0 ? Pro::NR : 1); r++) acc[r] = ((Pro::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  int plane = cid;
+  if (STAGED && warp == 0 && plane < N) issue(plane);
+  __syncthreads();
+
+  for (int it = 0; plane < N; plane += ncl, it++) {
+    const int next = plane + ncl;
+    if (STAGED) mbar_wait(bar, it & 1, &s_err);
+    {
+      const int j2 = tid & 7, r = tid >> 3;
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+      const T2 *row = STAGED ? stage + r * (N / 2) : reinterpret_cast<const T2 *>(src + rowoff);
+      T2 v[N1];
+      sfor<0, N1>([&](auto J1) {
+        constexpr int j1 = SPM_CI(J1);
+        const int j = j1 * 8 + j2;
+        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : __ldg(row + j), acc);
+      });
+      P::zf1_store(buf, ztw, v, r, j2);
+    }
+    __syncthreads();
+    if (STAGED && warp == 0 && next < N) {
+      fence_proxy_async();
+      issue(next);
+    }
+    P::zf2_post(buf, tw, tid, cluster);
+    P::yf(buf, tw, tid, rank, cluster, dst, plane);
     __syncthreads();
   }
   report_error(p, s_err);
@@ -482,7 +664,8 @@ template <int N, class T, class Epi, int CPS>
 __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
-  constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
+  using P = Plane<N, T>;
+  constexpr int M = G::M;
   constexpr bool STAGED = (CPS == 1);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
@@ -495,7 +678,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   if (flow_stopped(p)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
@@ -508,9 +691,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     s_err = 0;
     fence_barrier_init();
   }
-  for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
-  __syncthreads();
-  for (int i = tid; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
+  plane_twiddles<N, T>(p, tw, ztw);
   double acc[Epi::NR > 0 ? Epi::NR : 1];
 #pragma unroll
   for (int r = 0; r < (Epi::NR > 0 ? Epi::NR : 1); r++) acc[r] = ((Epi::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
@@ -518,135 +699,25 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   if (STAGED && tid == 0 && plane < N) issue(plane);
   __syncthreads();
   const T2 *gsrc = reinterpret_cast<const T2 *>(p.in[b]);
+  T *outb = reinterpret_cast<T *>(p.out[b]);  // null: reductions only
 
   for (int it = 0; plane < N; plane += ncl, it++) {
     const int next = plane + ncl;
     if (STAGED) mbar_wait(bar, it & 1, &s_err);
-    // ---- inverse y, stage 1: task (c, j2), input ky = 16*j1 + j2 (natural order)
-    {
-      const int c = tid & 15, j2 = tid >> 4;
-      T2 v[M1];
-      sfor<0, M1>([&](auto J1) {
-        constexpr int j1 = SPM_CI(J1);
-        v[j1] = STAGED ? stage[(16 * j1 + j2) * 16 + c]
-                       : __ldg(gsrc + ((size_t)plane * N + (16 * j1 + j2)) * M + rank * kCols + c);
-      });
-      Dft<+1, M1, T2>::run(v);
-      sfor<0, M1>([&](auto K1) {
-        constexpr int k1 = SPM_CI(K1);
-        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
-      });
-    }
-    __syncthreads();
+    P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
+      return STAGED ? stage[ky * 16 + c] : __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
+    });
     if (STAGED && tid == 0 && next < N) {
       fence_proxy_async();
       issue(next);
     }
-    // ---- inverse y, stage 2: task (c, k1) -> y = k1 + M1*k2; keep [y][c] in smem
-    {
-      T2 u[16];
-      const int c = tid & 15, k1 = tid >> 4;
-      if (tid < 16 * M1) {
-#pragma unroll
-        for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
-        Dft<+1, 16, T2>::run(u);
-      }
-      __syncthreads();
-      if (tid < 16 * M1) {
-#pragma unroll
-        for (int k2 = 0; k2 < 16; k2++) buf[(k1 + M1 * k2) * 16 + c] = u[k2];
-      }
-    }
-    cluster.sync();
-    // ---- complex-to-real pre-processing: gather the pairs (q, M-q) of my rows
-    {
-      constexpr int NT = kRows * (M / 2);
-      constexpr int TPT = NT / kThreads;  // N/32 tasks per thread
-      static_assert(NT % kThreads == 0, "task count");
-      T2 za[TPT], zb[TPT];
-#pragma unroll
-      for (int i = 0; i < TPT; i++) {
-        const int task = tid + i * kThreads;
-        const int r = task / (M / 2), q = task % (M / 2);
-        const int y = rank * kRows + r;
-        if (q == 0) {
-          const T2 *r0 = cluster.map_shared_rank(buf, 0u);
-          const T2 *rh = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols));
-          const T2 P = r0[y * 16 + 0];
-          const T2 a = rh[y * 16 + (M / 2) % kCols];
-          // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
-          za[i] = T2{P.x + P.y, P.x - P.y};
-          // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
-          const T2 e = {a.x + a.x, (T)0};
-          const T2 o = {(T)0, a.y + a.y};
-          zb[i] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
-        } else {
-          const T2 *ra = cluster.map_shared_rank(buf, (unsigned)(q / kCols));
-          const T2 *rb = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols));
-          const T2 a = ra[y * 16 + q % kCols];
-          const T2 c = rb[y * 16 + (M - q) % kCols];
-          // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
-          const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
-          const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
-          za[i] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
-          zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
-        }
-      }
-      cluster.sync();
-#pragma unroll
-      for (int i = 0; i < TPT; i++) {
-        const int task = tid + i * kThreads;
-        const int r = task / (M / 2), q = task % (M / 2);
-        T2 *Z = buf + r * M;
-        if (q == 0) {
-          Z[0] = za[i];
-          Z[M / 2] = zb[i];
-        } else {
-          Z[q] = za[i];
-          Z[M - q] = zb[i];
-        }
-      }
-    }
-    __syncthreads();
-    // ---- inverse z, stage 1: task (r, j2), element j = j1*8 + j2
-    {
-      const int j2 = tid & 7, r = tid >> 3;
-      T2 v[N1];
-      sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
-      __syncthreads();
-      Dft<+1, N1, T2>::run(v);
-      T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
-      sfor<0, N1>([&](auto K1) {
-        constexpr int k1 = SPM_CI(K1);
-        E[k1] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
-      });
-    }
-    __syncthreads();
-    // ---- inverse z, stage 2: task (r, k1) -> j = k1 + N1*k2; z_j = y_{2j} + i y_{2j+1}
-    {
-      constexpr int NT = kRows * N1;
-      constexpr int TPT = (NT + kThreads - 1) / kThreads;
-#pragma unroll
-      for (int t2 = 0; t2 < TPT; t2++) {
-        const int task = tid + t2 * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
-          T2 u[8];
-#pragma unroll
-          for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
-          Dft<+1, 8, T2>::run(u);
-          const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
-          T *outb = reinterpret_cast<T *>(p.out[b]);  // null: reductions only
-          T2 *dst = reinterpret_cast<T2 *>(outb + rowoff);
-#pragma unroll
-          for (int k2 = 0; k2 < 8; k2++) {
-            const int j = k1 + N1 * k2;
-            const T2 val = Epi::epi(p, b, rowoff + 2 * j, u[k2], acc);
-            if (outb) dst[j] = val;
-          }
-        }
-      }
-    }
+    P::c2r_pre(buf, tw, tid, rank, cluster);
+    P::zi1(buf, ztw, tid);
+    P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+      const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, acc);
+      if (outb) reinterpret_cast<T2 *>(outb + rowoff)[j] = val;
+    });
     __syncthreads();
   }
   report_error(p, s_err);
@@ -655,6 +726,103 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     if (grid_reduce<Epi::NR, Epi::MAXM>(acc, red, p.partials + (size_t)b * kPartStride * kRedMax,
                                         p.tickets + b, gridDim.x, blockIdx.x, tot))
       Epi::fin(p, b, tot);
+  }
+}
+
+// --------------------------------------------------------------- plane_inv_fwd
+// One x-plane pass that joins a step's inverse plane transform with the next
+// step's forward one: B (p.in, the spectrum of the pencil pass) -> inverse y,
+// C2R z -> epilogue -> phi rows kept in shared memory -> prologue -> R2C z,
+// y -> A (p.out). phi itself goes to memory (p.sto) only on the step where the
+// flow stops (the pencil pass armed FW_PENDING): the forward half is then
+// skipped. A chain of K steps is plane_fwd, K pencils, K-1 of these and one
+// plane_inv, so the real field crosses HBM once per chain instead of twice per
+// step. Direct loads, two CTAs per SM (the CPS = 2 layout).
+template <int N, class T, class Epi, class Pro>
+__global__ void __launch_bounds__(kThreads, 2) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
+  using G = Geo<N>;
+  using T2 = c2<T>;
+  using P = Plane<N, T>;
+  constexpr int M = G::M, N1 = G::N1;
+  constexpr int NE = Epi::NR, NP = Pro::NR, NA = (NE + NP > 0) ? NE + NP : 1;
+  static_assert(NA <= kRedMax, "reduction count");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
+  T2 *ztw = tw + N;
+  T2 *buf = ztw + N / 2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(buf + G::PLANE_UNITS);
+  double *red = reinterpret_cast<double *>(bar + 2);
+  if (flow_stopped(p)) return;
+  // uniform over the grid: set by the pencil pass of this step, before launch
+  const bool stop = p.flow != nullptr && *((volatile const int *)p.flow + FW_PENDING) != 0;
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int tid = threadIdx.x;
+  const int b = blockIdx.y;
+  const int rank = (int)cluster.block_rank();
+  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  plane_twiddles<N, T>(p, tw, ztw);
+  double acc_e[NE > 0 ? NE : 1], acc_p[NP > 0 ? NP : 1];
+#pragma unroll
+  for (int r = 0; r < (NE > 0 ? NE : 1); r++) acc_e[r] = ((Epi::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+#pragma unroll
+  for (int r = 0; r < (NP > 0 ? NP : 1); r++) acc_p[r] = ((Pro::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  __syncthreads();
+  const T2 *gsrc = reinterpret_cast<const T2 *>(p.in[b]);
+  T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
+  T *phi = reinterpret_cast<T *>(p.sto[b]);
+
+  for (int plane = cid; plane < N; plane += ncl) {
+    P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
+      return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
+    });
+    P::c2r_pre(buf, tw, tid, rank, cluster);
+    P::zi1(buf, ztw, tid);
+    if (stop) {
+      P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        reinterpret_cast<T2 *>(phi + rowoff)[j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
+      });
+    } else {
+      // phi rows [r][M] in buf
+      P::template zi2<true>(buf, tid, [&](int r, int j, T2 z) {
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        buf[r * M + j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
+      });
+      __syncthreads();
+      {
+        const int j2 = tid & 7, r = tid >> 3;
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        T2 v[N1];
+        sfor<0, N1>([&](auto J1) {
+          constexpr int j1 = SPM_CI(J1);
+          const int j = j1 * 8 + j2;
+          v[j1] = Pro::pro(p, b, rowoff + 2 * j, buf[r * M + j], acc_p);
+        });
+        __syncthreads();  // every row is read before the z exchange overwrites it
+        P::zf1_store(buf, ztw, v, r, j2);
+      }
+      __syncthreads();
+      P::zf2_post(buf, tw, tid, cluster);
+      P::yf(buf, tw, tid, rank, cluster, dst, plane);
+    }
+    __syncthreads();
+  }
+  double all[NA], tot[NA];
+#pragma unroll
+  for (int r = 0; r < NE; r++) all[r] = acc_e[r];
+#pragma unroll
+  for (int r = 0; r < NP; r++) all[NE + r] = acc_p[r];
+  if constexpr (NE + NP == 0) all[0] = 0.0;
+  if (grid_reduce<NA, (Epi::MAXM | (Pro::MAXM << NE))>(all, red, p.partials + (size_t)b * kPartStride * kRedMax,
+                                                        p.tickets + b, gridDim.x, blockIdx.x, tot)) {
+    double te[NE > 0 ? NE : 1], tp[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int r = 0; r < NE; r++) te[r] = tot[r];
+#pragma unroll
+    for (int r = 0; r < NP; r++) tp[r] = tot[NE + r];
+    Epi::fin(p, b, te);
+    if (!stop) Pro::fin(p, b, tp);
   }
 }
 

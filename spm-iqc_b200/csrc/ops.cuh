@@ -23,9 +23,13 @@ template <class T> struct ProIdent {
 //   nonlinear force  f(u) = Tau u + Gamma u^2 - u^3 = u (Tau + u (Gamma - u))
 //   energy density   e(u) = -Tau/2 u^2 - Gamma/3 u^3 + u^4/4
 //                         = u^2 (-Tau/2 + u (-Gamma/3 + u/4))
-template <class T> __device__ __forceinline__ T poly_force(T u, T tau, T gam) { return u * (tau + u * (gam - u)); }
+// (The outer products are rounded explicitly so that no kernel contracts them
+// into the sums that follow.)
+template <class T> __device__ __forceinline__ T poly_force(T u, T tau, T gam) {
+  return mul_rn(u, fma_rn(u, gam - u, tau));
+}
 template <class T> __device__ __forceinline__ T poly_energy(T u, T mtau2, T mgam3) {
-  return (u * u) * (mtau2 + u * (mgam3 + (T)0.25 * u));
+  return mul_rn(mul_rn(u, u), fma_rn(u, fma_rn((T)0.25, u, mgam3), mtau2));
 }
 
 // Gradient step (LPsrc.cpp:44-75): transform f(u) and sum the energy density.

@@ -85,6 +85,12 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
   for (int b = 0; b < nb; b++) SPM_TRY(spm_tensor_map(c, p.in[b], TM_PLANE_INV, &p.tmi[b]));
   return launch_cluster<Tag1, N>(c, plane_inv_kernel<N, T, Epi, 1>, plane_smem<N, T, 1>(), p, nb, "plane_inv");
 }
+// The fused inverse -> forward plane pass (direct loads, two CTAs per SM).
+template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
+  struct Tag {};
+  return launch_cluster<Tag, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro>, plane_smem<N, T, 2>(), p, nb,
+                                "plane_inv_fwd");
+}
 // Persistent pencil launch: resident CTAs (queried once), at most one per tile.
 template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p0, int nb) {
   KParams p = p0;
@@ -191,6 +197,46 @@ template <int N, class T> struct Impl {
     return 0;
   }
   static int grad_step(spm_ctx *c, void *phi, void *uhat) { return grad_step_ev(c, phi, uhat, nullptr); }
+
+  // K gated steps as one chain: plane_fwd, then per step a pencil pass and
+  // the fused inverse -> forward plane pass (the last step ends with
+  // plane_inv), so phi is read and written once per chain.
+  static int grad_steps(spm_ctx *c, void *phi, void *uhat, int K) {
+    if (K <= 0) return 0;
+    if (!c->fuse_planes || K == 1) {
+      for (int k = 0; k < K; k++) SPM_TRY(grad_step(c, phi, uhat));
+      return 0;
+    }
+    KParams p = spm_params(c);
+    p.flow = c->flow;
+    p.stats = c->stats;
+    p.in[0] = phi;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProGrad<T>>(c, p, 1)));
+    for (int k = 0; k < K; k++) {
+      KParams q = spm_params(c);
+      q.flow = c->flow;
+      q.stats = c->stats;
+      q.in[0] = spm_bufA(c, 0);
+      q.st[0] = uhat;
+      q.sto[0] = uhat;
+      q.out[0] = spm_bufB(c, 0);
+      SPM_TRY((pencil<N, T, OpGrad<T>>(c, q, 1)));
+      KParams r = spm_params(c);
+      r.flow = c->flow;
+      r.stats = c->stats;
+      r.in[0] = spm_bufB(c, 0);
+      if (k + 1 < K) {
+        r.out[0] = spm_bufA(c, 0);
+        r.sto[0] = phi;
+        SPM_TRY((plane_inv_fwd<N, T, EpiFlow<T>, ProGrad<T>>(c, r, 1)));
+      } else {
+        r.out[0] = phi;
+        SPM_TRY((plane_inv<N, T, EpiFlow<T>>(c, r, 1)));
+      }
+    }
+    return 0;
+  }
 
   // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
   static int ngrad(spm_ctx *c, const void *phi, void *grad) {
@@ -317,7 +363,7 @@ template <int N, class T> struct Impl {
   }
 
   static const OpsTable *table() {
-    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_step_ev, &ngrad, &hv, &precond, &dot,
+    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_step_ev, &ngrad, &hv, &precond, &dot,
                                &tangent, &force, &gnorm};
     return &t;
   }

@@ -307,12 +307,18 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->plane_cps = value;
     return SPM_OK;
   }
+  if (std::strcmp(knob, "fuse_planes") == 0) {
+    if (value != 0 && value != 1) return spm_fail(SPM_ERR_ARG, "fuse_planes must be 0 or 1");
+    c->fuse_planes = value;
+    return SPM_OK;
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
 extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (!c || !knob) return -1;
   if (std::strcmp(knob, "plane_cps") == 0) return c->plane_cps;
+  if (std::strcmp(knob, "fuse_planes") == 0) return c->fuse_planes;
   return -1;
 }
 
@@ -417,7 +423,7 @@ extern "C" int spm_grad_flow_enqueue(spm_ctx *c, void *phi, void *uhat, int nste
   const OpsTable *t = spm_table_of(c);
   c->m.tol_grad = tol_grad;
   int rc = SPM_OK;
-  for (int i = 0; i < nsteps && rc == SPM_OK; i++) rc = t->grad_step(c, phi, uhat);
+  rc = t->grad_steps(c, phi, uhat, nsteps);
   c->m.tol_grad = 0.0;
   return rc;
 }
@@ -456,7 +462,7 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
   cudaError_t e = cudaSuccess;
   while (enq < max_steps) {
     const int n = std::min(chunk, max_steps - enq);
-    for (int i = 0; i < n && rc == SPM_OK; i++) rc = t->grad_step(c, phi, uhat);
+    rc = t->grad_steps(c, phi, uhat, n);
     if (rc != SPM_OK) break;
     enq += n;
     e = cudaMemcpyAsync(c->host_flow, c->flow, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream);
@@ -481,6 +487,7 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->stream = c->stream;
   c->twin->cancel = c->cancel;
   c->twin->plane_cps = c->plane_cps;
+  c->twin->fuse_planes = c->fuse_planes;
   return SPM_OK;
 }
 

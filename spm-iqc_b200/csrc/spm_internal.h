@@ -49,6 +49,7 @@ struct spm_ctx {
   double *gtab = nullptr;       // spectral symbols per K^2 (4 doubles each)
   std::vector<TmEntry> tmaps;   // tensor-map cache (most recent last)
   int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
+  int fuse_planes = 1;          // gradient chains use the fused inverse -> forward plane pass
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
   const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)

@@ -111,3 +111,24 @@ def test_inpfp(spm, cuda):
     ctx = spm.SpmContext(N)
     a, b = npo.uniform_field(N, 1), npo.uniform_field(N, 2)
     assert abs(ctx.inpfp(t(cuda, a), t(cuda, b)) - m.inpfp(a, b)) <= 1e-12 * abs(m.inpfp(a, b))
+
+
+@pytest.mark.parametrize("N", [32, 64, 128, 160, 192])
+def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
+    """Chains of steps with the fused inverse -> forward plane pass give the
+    same bits (records, phi, u) as three passes per step, also when the flow
+    stops inside a chain (tol_grad reached mid-chunk)."""
+    phi = npo.uniform_field(N, 31)
+    out = []
+    for fuse in (0, 1):
+        ctx = spm.SpmContext(N, Tau=-0.02)
+        ctx.tune("fuse_planes", fuse)
+        pd = t(cuda, phi)
+        uh = ctx.my_fft(pd)
+        a = ctx.get_min_u_F(pd, uh, 37)
+        b = ctx.get_min_u_F(pd, uh, 3000, tol_grad=float(a[-1, 2]) * 0.3)
+        out.append((a, b, pd.cpu().numpy(), uh.cpu().numpy()))
+    (a0, b0, p0, u0), (a1, b1, p1, u1) = out
+    assert len(b0) < 3000 and len(b0) == len(b1)
+    assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
+    assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
