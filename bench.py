@@ -4,7 +4,8 @@ Workload (one "step" = one get_min_u_F iteration, LPsrc.cpp:52-110, with its
 energy, res and ||grad F|| reductions): N = 256, L = 26, Tau = -0.0061,
 Gamma = 0.30, dt = 0.3, phi0 = 0.15 * sum over the 30 icosahedral shell vectors
 of cos(2 pi n.x/N + theta) + N(0, 1e-3^2) noise (seeded). Fields stay in HBM;
-each step touches 1.07 GB (> the 126 MB L2), so no L2 flush is needed.
+each step moves 0.81 GB (6 fields) through HBM, well above the 126 MB L2, so no
+L2 flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,6 +35,22 @@ L, TAU, GAMMA, DT = 26.0, -0.0061, 0.30, 0.3
 METRIC = "N=256^3 grad-flow steps/s (FP64)"
 WORKLOAD = ("grad-flow 256^3 FP64, L=26, Tau=-0.0061, Gamma=0.30, dt=0.3, phi0 = icosahedral "
             "30-vector cosine shell (amp 0.15) + N(0,1e-3) noise")
+
+
+def kernel_traffic():
+    """DRAM bytes per launch of the step kernels at 256^3 FP64, from the ncu
+    capture summarised in profiles/kernel_traffic_256_fp64.md (lines
+    `traffic <kernel> <bytes>`)."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "kernel_traffic_256_fp64.md")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "traffic":
+                    out[parts[1]] = int(parts[2])
+    except OSError:
+        pass
+    return out
 
 
 def peaks():
@@ -183,7 +200,7 @@ def _serve_run(specs, fields, precision_of, slots, tol):
             time.sleep(delay)
         prec = precision_of(s.kind)
         d = spmiqc.job_desc(s.kind, s.N, prec, k=4, max_steps=SERVE_CAPS[s.kind], L=s.L, Tau=s.Tau, tol=tol,
-                            switch_tol=1e-6 if prec == "mixed" else 0.0, seed=s.seed)
+                            switch_tol=0.0, seed=s.seed)
         ids.append(srv.submit(d, p0, p1))
     res = [srv.wait(i, field=False)[0] for i in ids]
     st = srv.stats()
@@ -330,16 +347,21 @@ def main():
     lat = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(200))
     p50, p99 = lat[100], lat[197]
 
-    # per-kernel durations -> roofline of the dominant (pencil) pass
-    kms = (ctypes.c_double * 3)()
+    # per-kernel durations of the chain the timed region runs (one plane_fwd,
+    # then per step pencil + fused plane pass, one plane_inv) -> roofline of
+    # the dominant per-step kernel. Algorithmic bytes per launch: pencil reads
+    # A and u, writes u' and B (4S); the fused plane pass reads B, writes A
+    # (2S); plane_fwd reads phi, writes A; plane_inv reads B, writes phi (2S).
+    kms = (ctypes.c_double * 4)()
     spmiqc.check(L_.spm_grad_step_profile(ctx.h, phi.data_ptr(), uh.data_ptr(), 50, kms))
     kms = list(kms)
     hbm, peak_kind = peaks()
-    kern_bytes = [2 * S, 4 * S, 2 * S]  # plane-fwd: phi in, A out; pencil: A, u in, u', B out; plane-inv: B in, phi out
-    dom = int(np.argmax(kms))
+    names = ["plane_fwd<ProGrad>", "pencil<OpGrad>", "plane_inv_fwd<EpiFlow,ProGrad>", "plane_inv<EpiFlow>"]
+    kern_bytes = [2 * S, 4 * S, 2 * S, 2 * S]
+    dom = 1 if kms[1] >= kms[2] else 2
     achieved = kern_bytes[dom] / (kms[dom] * 1e-3) / 1e9
-    step_bytes = sum(kern_bytes)
-    names = ["plane_fwd<ProGrad>", "pencil<OpGrad>", "plane_inv<EpiFlow>"]
+    step_bytes = (6 * args.steps + 2) * S / args.steps  # per step of the timed chain
+    traffic = kernel_traffic().get(names[dom])
 
     # Hessian-vector products, block of 8 (LOBPCG k = 8)
     V = torch.from_numpy(np.random.default_rng(5).standard_normal((8, N, N, N))).cuda()
@@ -387,7 +409,7 @@ def main():
                 st = ctx.get_min_u_F(a, ua, 30000, tol_grad=1e-8)
                 n32, n64 = 0, len(st)
             else:
-                st, n32, n64 = ctx.get_min_u_F_mixed(a, ua, 30000, tol_grad=1e-8, switch_tol=1e-6)
+                st, n32, n64 = ctx.get_min_u_F_mixed(a, ua, 30000, tol_grad=1e-8, switch_tol=0.0)
             torch.cuda.synchronize()
             dt_s = time.perf_counter() - t0
             runs[mode] = (dt_s, n32, n64, float(st[-1, 2]), ctx.get_Ene(a, ua), a)
@@ -396,7 +418,7 @@ def main():
             "workload": "256^3 relaxation from uniform [-0.1,0.1] (seed 77), L=26, Tau=-0.0061, to ||grad F|| <= 1e-8",
             "fp64_s": runs["fp64"][0], "mixed_s": runs["mixed"][0], "speedup": runs["fp64"][0] / runs["mixed"][0],
             "fp64_steps": runs["fp64"][2], "mixed_fp32_steps": runs["mixed"][1], "mixed_fp64_steps": runs["mixed"][2],
-            "switch_tol": 1e-6, "grad_norm_fp64": runs["fp64"][3], "grad_norm_mixed": runs["mixed"][3],
+            "switch": "FP32 to 1e-8 or its rounding floor, then FP64", "grad_norm_fp64": runs["fp64"][3], "grad_norm_mixed": runs["mixed"][3],
             "energy_fp64": e64, "energy_mixed": emx,
             "energy_diff_rel_to_initial": abs(e64 - emx) / abs(ctx.get_Ene(torch.from_numpy(pu).cuda(),
                                                                            ctx.my_fft(torch.from_numpy(pu).cuda()))),
@@ -441,7 +463,8 @@ def main():
             "kernels_ms": dict(zip(names, kms)),
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                         "algorithmic_bytes": kern_bytes[dom], "traffic": None,
+                         "algorithmic_bytes": kern_bytes[dom], "traffic": traffic,
+                         "traffic_source": "profiles/kernel_traffic_256_fp64.md (ncu dram__bytes per launch)",
                          "step_frac": (step_bytes / (ms_max / args.steps * 1e-3) / 1e9) / hbm},
             "clocks": clk,
             "gpu_launches": int(launches),

@@ -121,9 +121,12 @@ int spm_grad_flow(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol
 
 /* Mixed-precision get_min_u_F (no counterpart in the reference): on an FP64
  * context, runs the flow with FP32 transforms (FP64 reductions) until
- * ||grad F|| <= switch_tol, then continues in FP64 from that state (phi cast
- * to FP64, uhat = my_fft(phi)) until ||grad F|| <= tol_grad. stats (host, >=
- * max_steps records, may be NULL) receives the FP32 steps then the FP64 ones. */
+ * ||grad F|| <= max(switch_tol, tol_grad) or until 512 FP32 steps bring no
+ * new minimum of ||grad F|| (the FP32 rounding floor), then continues in FP64
+ * from that state (phi cast to FP64, uhat = my_fft(phi)) until
+ * ||grad F|| <= tol_grad. switch_tol = 0 runs FP32 as far as it goes. stats
+ * (host, >= max_steps records, may be NULL) receives the FP32 steps then the
+ * FP64 ones. */
 int spm_grad_flow_mixed(spm_ctx *ctx, void *phi, void *uhat, int max_steps, double tol_grad, double switch_tol,
                         spm_step_stats *stats, int *steps_fp32, int *steps_fp64);
 
@@ -152,9 +155,13 @@ int spm_grad_flow_collect(spm_ctx *ctx, spm_step_stats *stats, int max_records, 
 int spm_grad_flow_host(spm_ctx *ctx, void *phi_host, int max_steps, double tol_grad,
                        spm_step_stats *stats, int *steps_done);
 
-/* Runs reps ungated gradient steps with CUDA events between the three
- * transform passes; ms[0..2] receive the mean duration of the plane-forward,
- * pencil and plane-inverse kernels. (Measurement aid; phi/uhat advance.) */
+/* Measurement aid (phi/uhat advance): runs reps >= 2 ungated gradient steps
+ * the way spm_grad_flow does, with CUDA events between the kernels. ms (4
+ * entries) receives the durations of plane_fwd (ms[0]), the mean pencil pass
+ * (ms[1]), the mean fused inverse -> forward plane pass (ms[2]; 0 with
+ * fuse_planes = 0) and plane_inv (ms[3]). With fuse_planes = 1 the steps form
+ * one chain (plane_fwd and plane_inv run once); with 0, every step runs all
+ * three passes and ms[0], ms[3] are means. */
 int spm_grad_step_profile(spm_ctx *ctx, void *phi, void *uhat, int reps, double *ms);
 
 /* ngrad_cam (LPsrc.cpp:119-173): grad = -grad F(phi). If norm is non-NULL it
@@ -203,7 +210,8 @@ int spm_spring_pairing(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double
                        int *iters);
 /* Mixed-precision Spring_Pairing (no counterpart in the reference): on an
  * FP64 context, the natural-force and min-max steps run with FP32 transforms
- * (FP64 reductions) until res <= switch_tol, then continue in FP64 from the
+ * (FP64 reductions) until res <= max(switch_tol, tol) or until 256 FP32
+ * iterations bring no new minimum of res, then continue in FP64 from the
  * cast replicas until res <= tol. res_hist (host, >= maxiter entries, may be
  * NULL) receives the FP32 iterations' residuals, then the FP64 ones. */
 int spm_spring_pairing_mixed(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double switch_tol,
@@ -256,7 +264,7 @@ typedef struct spm_job_desc {
   int reserved;
   double L, Tau, Gamma, dt;
   double tol;        /* ||grad F|| (relaxation), residual (LOBPCG, SPM) */
-  double switch_tol; /* SPM_MIXED: FP32 until this tolerance (0: 1e-6) */
+  double switch_tol; /* SPM_MIXED: FP32 until this tolerance (0: as far as FP32 goes) */
   uint64_t seed;     /* LOBPCG start block */
 } spm_job_desc;
 

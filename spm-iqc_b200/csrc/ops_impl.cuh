@@ -201,18 +201,26 @@ template <int N, class T> struct Impl {
   // K gated steps as one chain: plane_fwd, then per step a pencil pass and
   // the fused inverse -> forward plane pass (the last step ends with
   // plane_inv), so phi is read and written once per chain.
-  static int grad_steps(spm_ctx *c, void *phi, void *uhat, int K) {
+  // With ev non-null (2K + 2 events) the chain records ev[0] before the head,
+  // ev[1] after it and ev[2 + 2k], ev[3 + 2k] after step k's pencil and plane
+  // pass (for per-kernel timing).
+  static int grad_steps_ev(spm_ctx *c, void *phi, void *uhat, int K, void *const *ev) {
     if (K <= 0) return 0;
+    auto rec = [&](int i) {
+      if (ev) cudaEventRecord((cudaEvent_t)ev[i], c->stream);
+    };
     if (!c->fuse_planes || K == 1) {
       for (int k = 0; k < K; k++) SPM_TRY(grad_step(c, phi, uhat));
       return 0;
     }
+    rec(0);
     KParams p = spm_params(c);
     p.flow = c->flow;
     p.stats = c->stats;
     p.in[0] = phi;
     p.out[0] = spm_bufA(c, 0);
     SPM_TRY((plane_fwd<N, T, ProGrad<T>>(c, p, 1)));
+    rec(1);
     for (int k = 0; k < K; k++) {
       KParams q = spm_params(c);
       q.flow = c->flow;
@@ -222,6 +230,7 @@ template <int N, class T> struct Impl {
       q.sto[0] = uhat;
       q.out[0] = spm_bufB(c, 0);
       SPM_TRY((pencil<N, T, OpGrad<T>>(c, q, 1)));
+      rec(2 + 2 * k);
       KParams r = spm_params(c);
       r.flow = c->flow;
       r.stats = c->stats;
@@ -234,9 +243,11 @@ template <int N, class T> struct Impl {
         r.out[0] = phi;
         SPM_TRY((plane_inv<N, T, EpiFlow<T>>(c, r, 1)));
       }
+      rec(3 + 2 * k);
     }
     return 0;
   }
+  static int grad_steps(spm_ctx *c, void *phi, void *uhat, int K) { return grad_steps_ev(c, phi, uhat, K, nullptr); }
 
   // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
   static int ngrad(spm_ctx *c, const void *phi, void *grad) {
@@ -363,7 +374,7 @@ template <int N, class T> struct Impl {
   }
 
   static const OpsTable *table() {
-    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_step_ev, &ngrad, &hv, &precond, &dot,
+    static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_steps_ev, &grad_step_ev, &ngrad, &hv, &precond, &dot,
                                &tangent, &force, &gnorm};
     return &t;
   }

@@ -163,7 +163,7 @@ int run_job_gpu(spm_server *S, Job *j) {
     JOB_TRY(spm_fft(c, phi, uh));
     int n32 = 0, n64 = 0;
     if (mixed)
-      JOB_TRY(spm_grad_flow_mixed(c, phi, uh, d.max_steps, d.tol, d.switch_tol > 0 ? d.switch_tol : 1e-6, nullptr,
+      JOB_TRY(spm_grad_flow_mixed(c, phi, uh, d.max_steps, d.tol, d.switch_tol, nullptr,
                                   &n32, &n64));
     else
       JOB_TRY(spm_grad_flow(c, phi, uh, d.max_steps, d.tol, nullptr, &n64));
@@ -184,7 +184,7 @@ int run_job_gpu(spm_server *S, Job *j) {
     std::vector<double> hist((size_t)std::max(d.max_steps, 1));
     int n32 = 0, n64 = 0;
     if (mixed)
-      JOB_TRY(spm_spring_pairing_mixed(c, p0, p1, d.max_steps, d.tol, d.switch_tol > 0 ? d.switch_tol : 1e-6,
+      JOB_TRY(spm_spring_pairing_mixed(c, p0, p1, d.max_steps, d.tol, d.switch_tol,
                                        hist.data(), &n32, &n64));
     else
       JOB_TRY(spm_spring_pairing(c, p0, p1, d.max_steps, d.tol, hist.data(), &n64));

@@ -598,7 +598,23 @@ extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int 
   if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
   int n32 = 0, n64 = 0;
   const double sw = switch_tol > tol ? switch_tol : tol;
-  SPM_TRY(spm_spring_pairing(c->twin, a, b, maxiter, sw, res_hist, &n32));
+  // FP32 in windows of kWindow iterations until res <= sw, or until a window
+  // brings no new minimum of res (the FP32 rounding floor is reached)
+  constexpr int kWindow = 256;
+  std::vector<double> rec(kWindow);
+  double best = INFINITY;
+  while (n32 < maxiter) {
+    const int chunk = std::min(kWindow, maxiter - n32);
+    int done = 0;
+    double *out = res_hist ? res_hist + n32 : rec.data();
+    SPM_TRY(spm_spring_pairing(c->twin, a, b, chunk, sw, out, &done));
+    n32 += done;
+    if (done == 0 || done < chunk || out[done - 1] <= sw) break;
+    double wmin = INFINITY;
+    for (int i = 0; i < done; i++) wmin = std::min(wmin, out[i]);
+    if (!(wmin < best)) break;
+    best = wmin;
+  }
   c->launches += c->twin->launches + 2;
   c->twin->launches = 0;
   cast_kernel<float, double><<<1184, 256, 0, c->stream>>>(a, (double *)phi0, n);

@@ -510,7 +510,24 @@ extern "C" int spm_grad_flow_mixed(spm_ctx *c, void *phi, void *uhat, int max_st
   if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
   int n32 = 0, n64 = 0;
   const double sw = switch_tol > tol_grad ? switch_tol : tol_grad;
-  SPM_TRY(spm_grad_flow(c->twin, phi32, uh32, max_steps, sw, stats, &n32));
+  // FP32 in windows of kWindow steps until ||grad F|| <= sw, or until a window
+  // brings no new minimum of ||grad F|| (the FP32 rounding floor is reached).
+  constexpr int kWindow = 512;
+  std::vector<spm_step_stats> rec(kWindow);
+  double best = INFINITY;
+  while (n32 < max_steps) {
+    const int chunk = std::min(kWindow, max_steps - n32);
+    int done = 0;
+    spm_step_stats *out = stats ? stats + n32 : rec.data();
+    SPM_TRY(spm_grad_flow(c->twin, phi32, uh32, chunk, sw, out, &done));
+    n32 += done;
+    if (done == 0) break;
+    double wmin = INFINITY;
+    for (int i = 0; i < done; i++) wmin = std::min(wmin, out[i].grad_norm);
+    if (done < chunk || out[done - 1].grad_norm <= sw || out[done - 1].res <= 1e-16) break;
+    if (!(wmin < best)) break;
+    best = wmin;
+  }
   c->launches += c->twin->launches;
   c->twin->launches = 0;
   c->launches++;
@@ -543,29 +560,51 @@ extern "C" int spm_grad_flow_host(spm_ctx *c, void *phi_host, int max_steps, dou
 }
 
 extern "C" int spm_grad_step_profile(spm_ctx *c, void *phi, void *uhat, int reps, double *ms) {
-  if (!c || !phi || !uhat || !ms || reps < 1) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (!c || !phi || !uhat || !ms || reps < 2) return spm_fail(SPM_ERR_ARG, "bad argument (reps >= 2)");
   SPM_TRY(spm_ensure_scratch(c, 1));
   SPM_TRY(ensure_stats(c, reps));
   c->launches++;
   flow_init_kernel<<<1, 1, 0, c->stream>>>(c->flow);
+  const OpsTable *t = spm_table_of(c);
+  int rc = SPM_OK;
+  for (int k = 0; k < 4; k++) ms[k] = 0.0;
+  auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+    float f = 0;
+    cudaEventElapsedTime(&f, a, b);
+    return (double)f;
+  };
+  if (c->fuse_planes) {
+    // one chain: plane_fwd, reps x (pencil, plane_inv_fwd), the last plane pass plane_inv
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps + 2);
+    for (auto &e : ev) cudaEventCreate(&e);
+    rc = t->grad_steps_ev(c, phi, uhat, reps, (void *const *)ev.data());
+    if (rc == SPM_OK) {
+      cudaError_t e = cudaEventSynchronize(ev.back());
+      if (e != cudaSuccess) rc = spm_fail_cuda(e, "profile");
+    }
+    if (rc == SPM_OK) {
+      ms[0] = elapsed(ev[0], ev[1]);
+      for (int k = 0; k < reps; k++) ms[1] += elapsed(ev[1 + 2 * k], ev[2 + 2 * k]) / reps;
+      for (int k = 0; k + 1 < reps; k++) ms[2] += elapsed(ev[2 + 2 * k], ev[3 + 2 * k]) / (reps - 1);
+      ms[3] = elapsed(ev[2 * reps], ev[2 * reps + 1]);
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+  }
   cudaEvent_t ev[4];
   for (int i = 0; i < 4; i++) cudaEventCreate(&ev[i]);
   double acc[3] = {0, 0, 0};
-  int rc = SPM_OK;
-  const OpsTable *t = spm_table_of(c);
   for (int r = 0; r < reps && rc == SPM_OK; r++) {
     rc = t->grad_step_ev(c, phi, uhat, (void *const *)ev);
     if (rc != SPM_OK) break;
     cudaError_t e = cudaEventSynchronize(ev[3]);
     if (e != cudaSuccess) { rc = spm_fail_cuda(e, "profile"); break; }
-    for (int k = 0; k < 3; k++) {
-      float f = 0;
-      cudaEventElapsedTime(&f, ev[k], ev[k + 1]);
-      acc[k] += f;
-    }
+    for (int k = 0; k < 3; k++) acc[k] += elapsed(ev[k], ev[k + 1]);
   }
   for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
-  for (int k = 0; k < 3; k++) ms[k] = acc[k] / reps;
+  ms[0] = acc[0] / reps;
+  ms[1] = acc[1] / reps;
+  ms[3] = acc[2] / reps;
   return rc;
 }
 

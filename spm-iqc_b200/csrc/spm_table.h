@@ -11,6 +11,7 @@ struct OpsTable {
   int (*energy)(spm_ctx *, const void *phi, const void *uhat);
   int (*grad_step)(spm_ctx *, void *phi, void *uhat);
   int (*grad_steps)(spm_ctx *, void *phi, void *uhat, int nsteps);
+  int (*grad_steps_ev)(spm_ctx *, void *phi, void *uhat, int nsteps, void *const *events);
   int (*grad_step_ev)(spm_ctx *, void *phi, void *uhat, void *const *events);
   int (*ngrad)(spm_ctx *, const void *phi, void *grad);
   int (*hv)(spm_ctx *, const void *phi, const void *const *v, void *const *hv, int n);

@@ -217,8 +217,8 @@ class SpmContext:
                                   ctypes.byref(n)))
         return np.array([[s.energy, s.res, s.grad_norm, s.e1] for s in st[:n.value]]).reshape(-1, 4)
 
-    def get_min_u_F_mixed(self, phi, uhat, max_steps: int, tol_grad: float, switch_tol: float = 1e-6):
-        """FP32 flow to switch_tol, then FP64 polish to tol_grad (FP64 context).
+    def get_min_u_F_mixed(self, phi, uhat, max_steps: int, tol_grad: float, switch_tol: float = 0.0):
+        """FP32 flow to switch_tol (0: as far as FP32 goes), then FP64 polish to tol_grad (FP64 context).
         Returns (stats (n, 4), steps_fp32, steps_fp64)."""
         st = (StepStats * max(1, max_steps))()
         a, b = ctypes.c_int(), ctypes.c_int()
@@ -293,7 +293,7 @@ class SpmContext:
                                        ctypes.byref(it)))
         return np.array(hist[:it.value])
 
-    def Spring_Pairing_mixed(self, phi0, phi1, maxiter: int, tol: float, switch_tol: float = 1e-6):
+    def Spring_Pairing_mixed(self, phi0, phi1, maxiter: int, tol: float, switch_tol: float = 0.0):
         """FP32 iterations to switch_tol, then FP64 to tol; returns (history, fp32 iterations, fp64 iterations)."""
         hist = (ctypes.c_double * max(1, maxiter))()
         a, b = ctypes.c_int(), ctypes.c_int()

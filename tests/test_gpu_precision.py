@@ -85,3 +85,40 @@ def test_batched_flows_match_single_flows(cuda):
     for i in range(n):
         assert done[i] == singles[i][0], (i, done[i], singles[i][0])
         assert cuda.equal(phis[i], singles[i][1]), i
+
+
+def test_mixed_flow_fp32_as_far_as_it_goes(cuda):
+    """switch_tol = 0: the FP32 phase runs to the tolerance or to its rounding
+    floor; the FP64 polish then needs few steps, and the minimum matches the
+    all-FP64 one on the initial-energy scale."""
+    import spmiqc
+    N = 64
+    phi0 = npo.uniform_field(N, 22)
+    ctx = spmiqc.SpmContext(N)
+    a = cuda.from_numpy(phi0).cuda()
+    ua = ctx.my_fft(a)
+    E0 = ctx.get_Ene(a, ua)
+    sa = ctx.get_min_u_F(a, ua, 60000, tol_grad=1e-8)
+    b = cuda.from_numpy(phi0).cuda()
+    ub = ctx.my_fft(b)
+    sb, n32, n64 = ctx.get_min_u_F_mixed(b, ub, 60000, tol_grad=1e-8, switch_tol=0.0)
+    assert sa[-1, 2] <= 1e-8 and sb[-1, 2] <= 1e-8
+    assert n32 > 0.8 * len(sa) and n64 < 0.2 * len(sa), (n32, n64, len(sa))
+    assert abs(ctx.get_Ene(a, ua) - ctx.get_Ene(b, ub)) <= 1e-10 * abs(E0)
+
+
+def test_spring_pairing_fp32_phase_tracks_fp64(cuda):
+    """The FP32 phase of the mixed Spring_Pairing follows the FP64 iteration to
+    FP32 accuracy (20 iterations, no switch)."""
+    import spmiqc
+    N = 32
+    p0 = npo.uniform_field(N, 40)
+    p1 = p0 + 0.01 * npo.uniform_field(N, 41)
+    ctx = spmiqc.SpmContext(N)
+    a0, a1 = cuda.from_numpy(p0).cuda(), cuda.from_numpy(p1).cuda()
+    ha = ctx.Spring_Pairing(a0, a1, 20, 1e-30)
+    b0, b1 = cuda.from_numpy(p0).cuda(), cuda.from_numpy(p1).cuda()
+    hb, i32, i64 = ctx.Spring_Pairing_mixed(b0, b1, 20, 1e-30, switch_tol=0.0)
+    assert i32 == 20 and i64 == 0 and len(hb) == len(ha) == 20
+    assert np.max(np.abs(hb - ha) / ha) < 1e-4
+    assert rel(b0.cpu().numpy(), a0.cpu().numpy()) < 1e-5 and rel(b1.cpu().numpy(), a1.cpu().numpy()) < 1e-5
