@@ -457,7 +457,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "N": N, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (1.07 GB of fields per step)"},
+                       "l2": "inputs larger than L2 (0.81 GB of fields through HBM per step)"},
             "p50_ms": p50, "p99_ms": p99,
             "hv_per_s": hv_per_s, "fp32_steps_per_s": fp32_value, "precision": precision,
             "kernels_ms": dict(zip(names, kms)),
