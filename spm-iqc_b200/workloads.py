@@ -68,7 +68,10 @@ def field(spec: JobSpec, N: int | None = None, device: str | None = None) -> np.
     comes from torch's seeded generator), else by NumPy."""
     N = N or spec.N
     vec = shell_vectors(spec.shell, spec.L)
-    vec = vec[np.all(np.abs(vec) < N // 2, axis=1)]
+    # a shell beyond the grid's Nyquist range (small N, large L) is halved until it fits
+    while np.max(np.abs(vec)) >= N // 2:
+        vec = np.unique(np.round(vec / 2.0).astype(np.int64), axis=0)
+        vec = vec[np.any(vec != 0, axis=1)]
     amp = spec.amp * np.sqrt(2.0 / len(vec))
     if device is None:
         return inputs.cosine_shell(N, vec, amp=amp, seed=spec.seed, noise=1e-3)
