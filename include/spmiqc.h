@@ -237,6 +237,36 @@ int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
 int spm_inpfp_batch_noalloc(size_t n, int nb, int precision, const void *p, const void *q,
                             double *out, void *stream);
 
+/* ------------------------------------------------------------ field I/O */
+
+/* Save_phi / Save_Option_V (File_Op.cpp:8-49): count values of a host array,
+ * one per line as "%.16e \n" (k eigenvectors: k*N^3 values back to back). */
+int spm_save_field_txt(const char *path, const double *x, size_t count);
+/* load_phi / load_Option_V (File_Op.cpp:51-89): reads count values ("%lf");
+ * SPM_ERR_STATE if the file holds fewer. */
+int spm_load_field_txt(const char *path, double *x, size_t count);
+
+/* Binary checkpoint (no counterpart in the reference): nfields host fields of
+ * N^3 doubles with the model parameters and a step count; a checksum is
+ * verified on load. The file is written under a temporary name and renamed. */
+typedef struct spm_checkpoint_info {
+  int N, nfields, precision;
+  double L, Tau, Gamma, dt;
+  int64_t step;
+} spm_checkpoint_info;
+int spm_checkpoint_save(const char *path, const spm_checkpoint_info *info, const double *fields);
+/* fields may be NULL to read the header only; capacity in doubles. */
+int spm_checkpoint_load(const char *path, spm_checkpoint_info *info, double *fields, size_t capacity);
+
+/* get_initial_value (Initialization.cpp:242-339) on one initData file: full
+ * (host, 2*N^3 doubles, interleaved) receives the reference's u_F: 0.1 x the
+ * amplitude of each listed mode at k = round(k_file / l * L) (wrapped), where
+ * l is the shell scale the reference pairs with the phase (1 DIS/LAM, sqrt 2
+ * BCC/HPC, sqrt 3 FCC, sqrt 6 DG). */
+int spm_initdata_spectrum(const char *path, int N, double L, double l, double *full);
+/* The real initial field of that spectrum on the device: phi = Re(my_ifft(u_F)). */
+int spm_initial_field(spm_ctx *ctx, const char *path, double l, void *phi);
+
 /* ------------------------------------------------------------ job server */
 
 /* A job server (no counterpart in the reference, whose drivers run one job

@@ -22,6 +22,7 @@
 
 #include "BasicOperators.h"
 #include "Data.h"
+#include "File_Op.h"
 #include "Initialization.h"
 #include "LOBPCG.h"
 #include "LPsrc.h"
@@ -327,6 +328,76 @@ void ref_spring_pairing(double *phi0, double *phi1, double maxiter, double tol) 
   }
   to_real(Phi0[0], phi0);
   to_real(Phi0[1], phi1);
+}
+
+// File_Op.cpp:40-61 (Save_phi / load_phi) on a real field.
+void ref_save_phi(const double *phi, const char *path) {
+  Mute m;
+  const size_t n = (size_t)CplxDofs;
+  fftw_complex *x = (fftw_complex *)fftw_malloc(sizeof(fftw_complex) * n);
+  for (size_t i = 0; i < n; i++) {
+    x[i][0] = phi[i];
+    x[i][1] = 0.0;
+  }
+  Save_phi(x, const_cast<char *>(path));
+  fftw_free(x);
+}
+void ref_load_phi(const char *path, double *phi) {
+  Mute m;
+  const size_t n = (size_t)CplxDofs;
+  fftw_complex *x = (fftw_complex *)fftw_malloc(sizeof(fftw_complex) * n);
+  load_phi(x, const_cast<char *>(path));
+  for (size_t i = 0; i < n; i++) phi[i] = x[i][0];
+  fftw_free(x);
+}
+// File_Op.cpp:8-38, 63-89 (Save_Option_V / load_Option_V) on k fields.
+void ref_save_option_v(int k, const double *V, const char *path) {
+  Mute m;
+  Option opt;
+  memset(&opt, 0, sizeof(opt));
+  opt.k = k;
+  const size_t n = (size_t)CplxDofs_local;
+  opt.V = (fftw_complex **)malloc(sizeof(fftw_complex *) * k);
+  for (int i = 0; i < k; i++) {
+    opt.V[i] = (fftw_complex *)fftw_malloc(sizeof(fftw_complex) * n);
+    for (size_t j = 0; j < n; j++) {
+      opt.V[i][j][0] = V[i * n + j];
+      opt.V[i][j][1] = 0.0;
+    }
+  }
+  Save_Option_V(&opt, const_cast<char *>(path));
+  for (int i = 0; i < k; i++) fftw_free(opt.V[i]);
+  free(opt.V);
+}
+void ref_load_option_v(int k, const char *path, double *V) {
+  Mute m;
+  Option opt;
+  memset(&opt, 0, sizeof(opt));
+  opt.k = k;
+  const size_t n = (size_t)CplxDofs_local;
+  opt.V = (fftw_complex **)malloc(sizeof(fftw_complex *) * k);
+  for (int i = 0; i < k; i++) opt.V[i] = (fftw_complex *)fftw_malloc(sizeof(fftw_complex) * n);
+  load_Option_V(&opt, const_cast<char *>(path));
+  for (int i = 0; i < k; i++) {
+    for (size_t j = 0; j < n; j++) V[i * n + j] = opt.V[i][j][0];
+    fftw_free(opt.V[i]);
+  }
+  free(opt.V);
+}
+// get_initial_value (Initialization.cpp:242-339): reads ./initData/<phase>
+// relative to `root` (the directory holding initData/); uF_ri receives u_F.
+int ref_initial_value(int choice, const char *root, double *uF_ri) {
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(root) != 0) return 1;
+  const size_t n = (size_t)CplxDofs;
+  fftw_complex *u = (fftw_complex *)fftw_malloc(sizeof(fftw_complex) * n);
+  {
+    Mute m;
+    get_initial_value(u, choice, 0.0);
+  }
+  memcpy(uF_ri, u, sizeof(fftw_complex) * n);
+  fftw_free(u);
+  return chdir(cwd) == 0 ? 0 : 1;
 }
 
 }  // extern "C"

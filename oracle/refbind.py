@@ -61,6 +61,11 @@ def lib(path: str = LIB):
         L.ref_lobpcg_init.argtypes = [ctypes.c_int, ctypes.c_uint64, _dp]
         L.ref_lobpcg_inip.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp]
         L.ref_spring_pairing.argtypes = [_dp, _dp, ctypes.c_double, ctypes.c_double]
+        L.ref_save_phi.argtypes = [_dp, ctypes.c_char_p]
+        L.ref_load_phi.argtypes = [ctypes.c_char_p, _dp]
+        L.ref_save_option_v.argtypes = [ctypes.c_int, _dp, ctypes.c_char_p]
+        L.ref_load_option_v.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
+        L.ref_initial_value.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
         _libs[path] = L
     return _libs[path]
 
@@ -164,6 +169,32 @@ class Ref:
         b = np.array(phi1, dtype=np.float64, order="C")
         self.L.ref_spring_pairing(_p(a), _p(b), float(maxiter), float(tol))
         return a, b
+
+    # File_Op.cpp: the reference's field files
+    def save_phi(self, phi, path):
+        self.L.ref_save_phi(_p(np.ascontiguousarray(phi, dtype=np.float64)), path.encode())
+
+    def load_phi(self, path):
+        phi = self._z()
+        self.L.ref_load_phi(path.encode(), _p(phi))
+        return phi
+
+    def save_option_v(self, V, path):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        self.L.ref_save_option_v(V.shape[0], _p(V), path.encode())
+
+    def load_option_v(self, k, path):
+        V = self._z(k) if k > 1 else self._z()[None]
+        V = np.ascontiguousarray(V.reshape(k, self.N, self.N, self.N))
+        self.L.ref_load_option_v(k, path.encode(), _p(V))
+        return V
+
+    def initial_value(self, choice, root):
+        """get_initial_value: u_F of phase `choice` read from root/initData."""
+        u = np.zeros((self.N, self.N, self.N, 2))
+        if self.L.ref_initial_value(int(choice), root.encode(), _p(u)) != 0:
+            raise OSError("initial value: cannot enter " + root)
+        return u[..., 0] + 1j * u[..., 1]
 
     def close(self):
         self.L.ref_teardown()

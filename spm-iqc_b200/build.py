@@ -22,6 +22,7 @@ OBJ = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libspmiqc_cuda.so")
 COMPAT_LIB = os.path.join(LIBDIR, "libspmiqc_compat.so")
+BINDIR = os.path.join(HERE, "bin")
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -102,6 +103,18 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
             out = subprocess.run(cmd, capture_output=True, text=True)
             if out.returncode != 0:
                 raise RuntimeError("compat link failed:\n" + out.stderr[-4000:])
+    drivers = sorted(glob.glob(os.path.join(CSRC, "drivers", "*.cpp")))
+    if drivers:
+        os.makedirs(BINDIR, exist_ok=True)
+        for s in drivers:
+            exe = os.path.join(BINDIR, os.path.splitext(os.path.basename(s))[0])
+            if force or _stale(exe, [s, LIB] + headers):
+                cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                       "-I", os.path.join(CUDA_HOME, "include"), s, "-o", exe, "-L", LIBDIR, "-lspmiqc_cuda",
+                       "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN/../lib"]
+                out = subprocess.run(cmd, capture_output=True, text=True)
+                if out.returncode != 0:
+                    raise RuntimeError("driver build failed:\n" + out.stderr[-4000:])
     return LIB
 
 

@@ -301,6 +301,14 @@ class SpmContext:
                                              float(switch_tol), hist, ctypes.byref(a), ctypes.byref(b)))
         return np.array(hist[:a.value + b.value]), a.value, b.value
 
+    def initial_field(self, path: str, l: float, phi=None):
+        """get_initial_value of an initData file (shell scale l): phi = Re(my_ifft(u_F))."""
+        phi = self.field() if phi is None else phi
+        f = lib().spm_initial_field
+        f.argtypes = [_vp, ctypes.c_char_p, ctypes.c_double, _vp]
+        check(f(self.h, path.encode(), float(l), _ptr(phi)))
+        return phi
+
     # ---- BasicOperators.cpp
     def inpfp(self, p, q) -> float:
         out = ctypes.c_double()
@@ -399,3 +407,47 @@ class JobServer:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- field files
+def save_field_txt(path: str, x) -> None:
+    """Save_phi / Save_Option_V format ("%.16e \\n" per value) from a host array."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    f = lib().spm_save_field_txt
+    f.argtypes = [ctypes.c_char_p, _vp, ctypes.c_size_t]
+    check(f(path.encode(), a.ctypes.data, a.size))
+
+
+def load_field_txt(path: str, count: int) -> np.ndarray:
+    out = np.empty(int(count), dtype=np.float64)
+    f = lib().spm_load_field_txt
+    f.argtypes = [ctypes.c_char_p, _vp, ctypes.c_size_t]
+    check(f(path.encode(), out.ctypes.data, out.size))
+    return out
+
+
+class CheckpointInfo(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("nfields", ctypes.c_int), ("precision", ctypes.c_int),
+                ("L", ctypes.c_double), ("Tau", ctypes.c_double), ("Gamma", ctypes.c_double),
+                ("dt", ctypes.c_double), ("step", ctypes.c_int64)]
+
+
+def save_checkpoint(path: str, fields, L: float, Tau: float, Gamma: float, dt: float, step: int = 0,
+                    precision: int = SPM_FP64) -> None:
+    a = np.ascontiguousarray(fields, dtype=np.float64)
+    N = a.shape[-1]
+    info = CheckpointInfo(N, a.size // N ** 3, precision, L, Tau, Gamma, dt, step)
+    f = lib().spm_checkpoint_save
+    f.argtypes = [ctypes.c_char_p, _vp, _vp]
+    check(f(path.encode(), ctypes.byref(info), a.ctypes.data))
+
+
+def load_checkpoint(path: str):
+    """Returns (info, fields of shape (nfields, N, N, N))."""
+    info = CheckpointInfo()
+    f = lib().spm_checkpoint_load
+    f.argtypes = [ctypes.c_char_p, _vp, _vp, ctypes.c_size_t]
+    check(f(path.encode(), ctypes.byref(info), None, 0))
+    out = np.empty((info.nfields, info.N, info.N, info.N))
+    check(f(path.encode(), ctypes.byref(info), out.ctypes.data, out.size))
+    return info, out
