@@ -59,6 +59,16 @@ struct Opts {
     if (_rc != SPM_OK) die(#x, _rc); \
   } while (0)
 
+double num(const char *opt, const char *v) {
+  char *end = nullptr;
+  const double x = std::strtod(v, &end);
+  if (end == v || *end != '\0') {
+    std::fprintf(stderr, "spmiqc_drive: %s needs a number, got '%s'\n", opt, v);
+    std::exit(1);
+  }
+  return x;
+}
+
 double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -220,23 +230,23 @@ int main(int argc, char **argv) {
   for (int i = 2; i + 1 < argc; i += 2) {
     const std::string k = argv[i];
     const char *v = argv[i + 1];
-    if (k == "--N") o.N = std::atoi(v);
-    else if (k == "--L") o.L = std::atof(v);
-    else if (k == "--Tau") o.Tau = std::atof(v);
-    else if (k == "--Gamma") o.Gamma = std::atof(v);
-    else if (k == "--dt") o.dt = std::atof(v);
-    else if (k == "--max-iter") o.max_iter = std::atoi(v);
-    else if (k == "--tol-grad") o.tol_grad = std::atof(v);
+    if (k == "--N") o.N = (int)num(k.c_str(), v);
+    else if (k == "--L") o.L = num(k.c_str(), v);
+    else if (k == "--Tau") o.Tau = num(k.c_str(), v);
+    else if (k == "--Gamma") o.Gamma = num(k.c_str(), v);
+    else if (k == "--dt") o.dt = num(k.c_str(), v);
+    else if (k == "--max-iter") o.max_iter = (int)num(k.c_str(), v);
+    else if (k == "--tol-grad") o.tol_grad = num(k.c_str(), v);
     else if (k == "--init") o.init = v;
-    else if (k == "--l") o.l = std::atof(v);
+    else if (k == "--l") o.l = num(k.c_str(), v);
     else if (k == "--init-txt") o.init_txt = v;
     else if (k == "--result") o.result = v;
-    else if (k == "--lobpcg-calls") o.lobpcg_calls = std::atoi(v);
-    else if (k == "--lobpcg-calls2") o.lobpcg_calls2 = std::atoi(v);
-    else if (k == "--lobpcg-iters") o.lobpcg_iters = std::atoi(v);
-    else if (k == "--spm-maxiter") o.spm_maxiter = std::atoi(v);
-    else if (k == "--spm-tol") o.spm_tol = std::atof(v);
-    else if (k == "--seed") o.seed = std::strtoull(v, nullptr, 10);
+    else if (k == "--lobpcg-calls") o.lobpcg_calls = (int)num(k.c_str(), v);
+    else if (k == "--lobpcg-calls2") o.lobpcg_calls2 = (int)num(k.c_str(), v);
+    else if (k == "--lobpcg-iters") o.lobpcg_iters = (int)num(k.c_str(), v);
+    else if (k == "--spm-maxiter") o.spm_maxiter = (int)num(k.c_str(), v);
+    else if (k == "--spm-tol") o.spm_tol = num(k.c_str(), v);
+    else if (k == "--seed") o.seed = (unsigned long long)num(k.c_str(), v);
     else {
       std::fprintf(stderr, "spmiqc_drive: unknown option %s\n", k.c_str());
       return 1;

@@ -62,7 +62,7 @@ def test_driver_stages_match_oracle_replay(cuda, tmp_path):
     res.mkdir()
     common = ["--N", str(N), "--L", str(L), "--Tau", str(TAU), "--max-iter", "200", "--lobpcg-iters", "10",
               "--result", str(res)]
-    out1 = _run(["stage1"] + common + ["--init", init, "--l", repr(L_SHELL), "--lobpcg-calls", "2",
+    out1 = _run(["stage1"] + common + ["--init", init, "--l", f"{float(L_SHELL):.17g}", "--lobpcg-calls", "2",
                                        "--spm-maxiter", "10", "--spm-tol", "1e-12"], str(tmp_path))
     E = _energies(out1, "Energy of metastable state")[0]
     Es = _energies(out1, "Energy of transition state")[0]
