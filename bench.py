@@ -109,6 +109,8 @@ class Clocks:
 
 
 def dist_setup():
+    """One process per GPU (torchrun env). NCCL with a GPU; gloo on a CPU-only
+    host (the multi-rank logic is tested that way)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -116,9 +118,28 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if not dist.is_initialized():
+            if torch.cuda.is_available():
+                torch.cuda.set_device(local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            else:
+                dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return rank, world, local
+
+
+def _dev():
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
+def gather_over_ranks(items: list, world: int) -> list:
+    """Concatenation of every rank's list (same order of ranks on all ranks)."""
+    if world == 1:
+        return list(items)
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, list(items))
+    return [x for part in out for x in part]
 
 
 def barrier(world):
@@ -132,7 +153,7 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -188,12 +209,14 @@ def reference_arm(args, rank, world):
 SERVE_CAPS = {"relax": 4000, "lobpcg": 21, "spm": 300}
 
 
-def _serve_run(specs, fields, precision_of, slots, tol):
-    """Replays the arrival stream into a job server; returns per-job results and server stats."""
+def _serve_run(specs, fields, precision_of, slots, tol, fake=False, t0=None):
+    """Replays the arrival stream into a job server; returns per-job results and
+    server stats. fake: the server's fake device (scheduler only, no GPU)."""
     import spmiqc
-    srv = spmiqc.JobServer(max_slots=slots)
+    srv = (spmiqc.JobServer(budget_bytes=64 << 30, max_slots=slots, fake_device=True, fake_ms_per_munit=0.5)
+           if fake else spmiqc.JobServer(max_slots=slots))
     ids = []
-    t0 = time.perf_counter()
+    t0 = time.perf_counter() if t0 is None else t0
     for s, (p0, p1) in zip(specs, fields):
         delay = s.t_arrival - (time.perf_counter() - t0)
         if delay > 0:
@@ -208,6 +231,37 @@ def _serve_run(specs, fields, precision_of, slots, tol):
     return res, st
 
 
+def serve_ranks(specs, make_fields, rank, world, slots, precision_of, tol, fake=False):
+    """Runs this rank's share of the stream (jobs partitioned over the ranks by
+    device-memory footprint, arrival times kept) and returns the whole-job
+    aggregate on every rank: completed jobs of all ranks / the longest makespan,
+    latency percentiles over all jobs."""
+    import numpy as np
+    import workloads
+    mine = workloads.partition_jobs(specs, world)[rank]
+    sub = [specs[i] for i in mine]
+    fields = [make_fields(s) for s in sub]
+    barrier(world)
+    res, st = _serve_run(sub, fields, precision_of, slots, tol, fake=fake)
+    ok = [r for r in res if r.status == 0]
+    span = (max(r.t_end for r in res) - min(r.t_submit for r in res)) if res else 0.0
+    lat = gather_over_ranks([r.t_end - r.t_submit for r in ok], world)
+    fails = gather_over_ranks([f"{s.kind} N={s.N}: {r.message.decode()}" for s, r in zip(sub, res) if r.status != 0],
+                              world)
+    conv = {k: int(sum(1 for s, r in zip(sub, res) if s.kind == k and r.status == 0 and r.residual <= tol))
+            for k in SERVE_CAPS}
+    conv = {k: sum(c[k] for c in gather_over_ranks([conv], world)) for k in SERVE_CAPS}
+    completed = len(lat)
+    span = max_over_ranks(span, world)
+    lat = np.array(lat) if lat else np.zeros(1)
+    return {"failures": fails, "jobs_per_s": completed / span if span > 0 else 0.0,
+            "p50_s": float(np.percentile(lat, 50, method="inverted_cdf")),
+            "p99_s": float(np.percentile(lat, 99, method="inverted_cdf")), "completed": completed,
+            "failed": len(fails), "peak_running_rank0": int(st.peak_running),
+            "peak_reserved_gb_rank0": st.peak_bytes / 1e9, "makespan_s": span, "reached_tol": conv,
+            "jobs_per_rank": [len(p) for p in workloads.partition_jobs(specs, world)]}
+
+
 def serve_bench(args):
     """Serving workload: a seeded Poisson stream (mean 4 jobs/s) of 70%
     relaxations (FP32 + FP64 polish), 20% k=4 LOBPCG (FP64) and 10% SPM saddle
@@ -215,39 +269,37 @@ def serve_bench(args):
     job server with concurrent slots, next to the same stream executed serially
     in FP64 (one job at a time, as the reference's one-job-per-program
     drivers do)."""
-    import numpy as np
     import torch
     import workloads
-    torch.cuda.set_device(0)
-    specs = workloads.serving_stream(seed=2024, n_jobs=args.serve_jobs, rate=4.0)
-    fields = []
-    for s in specs:
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    specs = workloads.serving_stream(seed=2024, n_jobs=args.serve_jobs, rate=4.0 * world)
+
+    def make_fields(s):
         p = workloads.field(s, device="cuda")
-        fields.append(workloads.replicas(s, p) if s.kind == "spm" else (p, None))
-    torch.cuda.empty_cache()
+        return workloads.replicas(s, p) if s.kind == "spm" else (p, None)
+
     tol = 1e-8
     out = {}
     for name, slots, prec in (("served", args.serve_slots, lambda k: "fp64" if k == "lobpcg" else "mixed"),
                               ("serial_fp64", 1, lambda k: "fp64")):
-        res, st = _serve_run(specs, fields, prec, slots, tol)
-        ok = [r for r in res if r.status == 0]
-        span = max(r.t_end for r in res) - min(r.t_submit for r in res)
-        lat = np.array([r.t_end - r.t_submit for r in ok])
-        conv = {k: int(sum(1 for s, r in zip(specs, res) if s.kind == k and r.status == 0 and r.residual <= tol))
-                for k in SERVE_CAPS}
-        fails = [f"{s.kind} N={s.N}: {r.message.decode()}" for s, r in zip(specs, res) if r.status != 0]
-        out[name] = {"failures": fails, "jobs_per_s": len(ok) / span, "p50_s": float(np.percentile(lat, 50, method="inverted_cdf")),
-                     "p99_s": float(np.percentile(lat, 99, method="inverted_cdf")), "completed": len(ok),
-                     "failed": int(st.failed), "peak_running": int(st.peak_running),
-                     "peak_reserved_gb": st.peak_bytes / 1e9, "makespan_s": span, "reached_tol": conv}
+        out[name] = serve_ranks(specs, make_fields, rank, world, slots, prec, tol)
+        torch.cuda.empty_cache()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
     kinds = {k: sum(1 for s in specs if s.kind == k) for k in SERVE_CAPS}
     sizes = {str(n): sum(1 for s in specs if s.N == n) for n in (64, 128, 192, 256)}
     line = {"metric": "serving jobs/s (Poisson 4/s, 70% relax / 20% LOBPCG k=4 / 10% SPM)",
-            "value": out["served"]["jobs_per_s"], "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True,
+            "value": out["served"]["jobs_per_s"], "unit": "jobs/s", "n_gpus": world, "higher_is_better": True,
+            "scaling": "weak",
             "p50_s": out["served"]["p50_s"], "p99_s": out["served"]["p99_s"], "served": out["served"],
             "serial_fp64": out["serial_fp64"], "data": "synthetic",
             "config": {"workload": "serving stream", "jobs": len(specs), "kinds": kinds, "sizes": sizes,
-                       "caps": SERVE_CAPS, "tol": tol, "slots": args.serve_slots, "seed": 2024}}
+                       "caps": SERVE_CAPS, "tol": tol, "slots": args.serve_slots, "seed": 2024,
+                       "rate_per_s": 4.0 * world, "parallelism": f"jobs partitioned by footprint over {world} GPU(s)"}}
     print(json.dumps(line))
     return 0
 

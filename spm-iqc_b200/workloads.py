@@ -96,3 +96,25 @@ def replicas(spec: JobSpec, phi: np.ndarray):
     n = phi.shape[0]
     d = np.cos(2 * np.pi * m * np.arange(n) / n)
     return phi, phi + 0.01 * d[:, None, None]
+
+
+def job_bytes(spec: JobSpec) -> int:
+    """Device-memory footprint of the job as the job server admits it."""
+    import spmiqc
+    prec = "fp64" if spec.kind == "lobpcg" else "mixed"
+    return spmiqc.job_footprint(spmiqc.job_desc(spec.kind, spec.N, prec, k=4))
+
+
+def partition_jobs(specs, world: int):
+    """Jobs over `world` GPUs (no exchange between them): largest footprint
+    first, each to the GPU with the least total footprint so far (ties to the
+    lower rank). Deterministic, so every rank computes the same partition;
+    each rank's list is in arrival order."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    order = sorted(range(len(specs)), key=lambda i: (-job_bytes(specs[i]), i))
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += job_bytes(specs[i])
+    return [sorted(p) for p in parts]
