@@ -32,8 +32,7 @@ template <int N> struct Geo {
   static constexpr int CL = N / kRows;      // CTAs per cluster = per x-plane
   static constexpr int N1 = M / 8;          // z stage-1 radix (z stage-2 radix is 8)
   static constexpr int M1 = N / 16;         // y/x stage-1 radix (stage-2 radix is 16)
-  static constexpr int ZPAD = N1 + 1;       // padded k1 extent of the z exchange
-  static constexpr int PLANE_UNITS = kRows * 8 * ZPAD > kRows * M ? kRows * 8 * ZPAD : kRows * M;
+  static constexpr int PLANE_UNITS = kRows * M;  // = 16 N: 32 rows, or 16 columns x N
   static constexpr int PENCIL_UNITS = M1 * 16 * 16;   // = 16 N
   static constexpr int STAGE_UNITS = 16 * N;          // one staged tile (plane rows / columns / pencils)
   static constexpr int PTILES = (N / 2) * (M / 8);    // pencil tiles per field
@@ -75,52 +74,63 @@ template <int N, class T> struct Plane {
   using G = Geo<N>;
   using T2 = c2<T>;
   static constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
+  // The z phases of a row stay inside one warp: warp w owns rows
+  // RPW*w .. RPW*w + RPW - 1 in every z phase, and the z exchange of row r
+  // lies inside row r's own M units, so those phases need only warp barriers.
+  static constexpr int RPW = kRows / (kThreads / 32);
+  static_assert(RPW * 8 == 32, "8 threads per row in the row-parallel z stages");
+
+  // z-exchange slot of stage-1 output (j2, k1) of row r, rotated by j2 so the
+  // 8 threads of a row (and the 8 values a stage-2 task reads) fall in
+  // distinct bank groups.
+  __device__ static int zslot(int r, int j2, int k1) { return r * M + j2 * N1 + (k1 + j2) % N1; }
 
   // forward z, stage 1 of task (row r, j2): v = row elements j = j1*8 + j2
   // (after the prologue); radix-N1 DFT, twiddle, store into the z exchange.
   __device__ static void zf1_store(T2 *buf, const T2 *ztw, T2 (&v)[N1], int r, int j2) {
     Dft<-1, N1, T2>::run(v);
-    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
     sfor<0, N1>([&](auto K1) {
       constexpr int k1 = SPM_CI(K1);
-      E[k1] = (k1 == 0) ? v[k1] : cmul(v[k1], ztw[k1 * 8 + j2]);
+      buf[zslot(r, j2, k1)] = (k1 == 0) ? v[k1] : cmul(v[k1], ztw[k1 * 8 + j2]);
     });
   }
 
   // forward z, stage 2 (8-point DFTs over j2 -> k = k1 + N1*k2) and the
-  // real-to-complex post-processing of the packed lines (pairs q, M-q). Ends
-  // with a cluster barrier: the rows [r][M] are then ready for remote reads.
+  // real-to-complex post-processing of the packed lines (pairs q, M-q), each
+  // warp on its own rows. Ends with a cluster barrier: the rows [r][M] are
+  // then ready for remote reads.
   __device__ static void zf2_post(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster) {
+    const int warp = tid >> 5, lane = tid & 31;
     {
-      constexpr int NT = kRows * N1;
-      constexpr int TPT = (NT + kThreads - 1) / kThreads;
+      constexpr int NT = RPW * N1;  // tasks (r, k1) of this warp
+      constexpr int TPT = (NT + 31) / 32;
       T2 u[TPT][8];
 #pragma unroll
       for (int t = 0; t < TPT; t++) {
-        const int task = tid + t * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
+        const int q = lane + 32 * t;
+        if (q < NT) {
+          const int r = RPW * warp + q / N1, k1 = q % N1;
 #pragma unroll
-          for (int j2 = 0; j2 < 8; j2++) u[t][j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          for (int j2 = 0; j2 < 8; j2++) u[t][j2] = buf[zslot(r, j2, k1)];
         }
       }
-      __syncthreads();
+      __syncwarp();
 #pragma unroll
       for (int t = 0; t < TPT; t++) {
-        const int task = tid + t * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
+        const int q = lane + 32 * t;
+        if (q < NT) {
+          const int r = RPW * warp + q / N1, k1 = q % N1;
           Dft<-1, 8, T2>::run(u[t]);
 #pragma unroll
           for (int k2 = 0; k2 < 8; k2++) buf[r * M + k1 + N1 * k2] = u[t][k2];
         }
       }
     }
-    __syncthreads();
+    __syncwarp();
     {
-      constexpr int NT = kRows * (M / 2);
-      for (int task = tid; task < NT; task += kThreads) {
-        const int r = task / (M / 2), q = task % (M / 2);
+      constexpr int NT = RPW * (M / 2);
+      for (int task = lane; task < NT; task += 32) {
+        const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
         T2 *Z = buf + r * M;
         if (q == 0) {
           const T2 z0 = Z[0];
@@ -217,16 +227,18 @@ template <int N, class T> struct Plane {
   }
 
   // complex-to-real pre-processing: gather the pairs (q, M-q) of this CTA's
-  // rows from the column owners, then store the rows [r][M].
+  // rows from the column owners, then store the rows [r][M] (each warp its own
+  // rows, ready for zi1 of the same warp).
   __device__ static void c2r_pre(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster) {
-    constexpr int NT = kRows * (M / 2);
-    constexpr int TPT = NT / kThreads;  // N/32 tasks per thread
-    static_assert(NT % kThreads == 0, "task count");
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NT = RPW * (M / 2);
+    constexpr int TPT = NT / 32;  // N/32 tasks per thread
+    static_assert(NT % 32 == 0, "task count");
     T2 za[TPT], zb[TPT];
 #pragma unroll
     for (int i = 0; i < TPT; i++) {
-      const int task = tid + i * kThreads;
-      const int r = task / (M / 2), q = task % (M / 2);
+      const int task = lane + 32 * i;
+      const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
       const int y = rank * kRows + r;
       if (q == 0) {
         const T2 *r0 = cluster.map_shared_rank(buf, 0u);
@@ -254,8 +266,8 @@ template <int N, class T> struct Plane {
     cluster.sync();
 #pragma unroll
     for (int i = 0; i < TPT; i++) {
-      const int task = tid + i * kThreads;
-      const int r = task / (M / 2), q = task % (M / 2);
+      const int task = lane + 32 * i;
+      const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
       T2 *Z = buf + r * M;
       if (q == 0) {
         Z[0] = za[i];
@@ -265,39 +277,40 @@ template <int N, class T> struct Plane {
         Z[M - q] = zb[i];
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
 
-  // inverse z, stage 1 of task (r, j2): rows [r][M] -> z exchange.
+  // inverse z, stage 1 of task (r, j2): row r -> its z exchange (same warp).
   __device__ static void zi1(T2 *buf, const T2 *ztw, int tid) {
     const int j2 = tid & 7, r = tid >> 3;
     T2 v[N1];
     sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
-    __syncthreads();
+    __syncwarp();
     Dft<+1, N1, T2>::run(v);
-    T2 *E = buf + r * (8 * G::ZPAD) + j2 * G::ZPAD;
     sfor<0, N1>([&](auto K1) {
       constexpr int k1 = SPM_CI(K1);
-      E[k1] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
+      buf[zslot(r, j2, k1)] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
     });
-    __syncthreads();
+    __syncwarp();
   }
 
-  // inverse z, stage 2 of task (r, k1): 8-point DFTs; sink(r, j, z_j) gets
-  // z_j = y_{2j} + i y_{2j+1}, j = k1 + N1*k2. With TO_SMEM the sink may
-  // overwrite buf: every task is read first, then a barrier, then the sinks.
+  // inverse z, stage 2 of task (r, k1) of this warp's rows: 8-point DFTs;
+  // sink(r, j, z_j) gets z_j = y_{2j} + i y_{2j+1}, j = k1 + N1*k2. With
+  // TO_SMEM the sink may overwrite the warp's rows in buf: every task is read
+  // first, then a warp barrier, then the sinks.
   template <bool TO_SMEM, class SINK> __device__ static void zi2(T2 *buf, int tid, SINK sink) {
-    constexpr int NT = kRows * N1;
-    constexpr int TPT = (NT + kThreads - 1) / kThreads;
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NT = RPW * N1;
+    constexpr int TPT = (NT + 31) / 32;
     if constexpr (!TO_SMEM) {
 #pragma unroll
       for (int t2 = 0; t2 < TPT; t2++) {
-        const int task = tid + t2 * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
+        const int q = lane + 32 * t2;
+        if (q < NT) {
+          const int r = RPW * warp + q / N1, k1 = q % N1;
           T2 u[8];
 #pragma unroll
-          for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          for (int j2 = 0; j2 < 8; j2++) u[j2] = buf[zslot(r, j2, k1)];
           Dft<+1, 8, T2>::run(u);
 #pragma unroll
           for (int k2 = 0; k2 < 8; k2++) sink(r, k1 + N1 * k2, u[k2]);
@@ -307,20 +320,20 @@ template <int N, class T> struct Plane {
       T2 u[TPT][8];
 #pragma unroll
       for (int t2 = 0; t2 < TPT; t2++) {
-        const int task = tid + t2 * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
+        const int q = lane + 32 * t2;
+        if (q < NT) {
+          const int r = RPW * warp + q / N1, k1 = q % N1;
 #pragma unroll
-          for (int j2 = 0; j2 < 8; j2++) u[t2][j2] = buf[r * (8 * G::ZPAD) + j2 * G::ZPAD + k1];
+          for (int j2 = 0; j2 < 8; j2++) u[t2][j2] = buf[zslot(r, j2, k1)];
           Dft<+1, 8, T2>::run(u[t2]);
         }
       }
-      __syncthreads();
+      __syncwarp();
 #pragma unroll
       for (int t2 = 0; t2 < TPT; t2++) {
-        const int task = tid + t2 * kThreads;
-        if (task < NT) {
-          const int r = task / N1, k1 = task % N1;
+        const int q = lane + 32 * t2;
+        if (q < NT) {
+          const int r = RPW * warp + q / N1, k1 = q % N1;
 #pragma unroll
           for (int k2 = 0; k2 < 8; k2++) sink(r, k1 + N1 * k2, u[t2][k2]);
         }
@@ -402,7 +415,8 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       });
       P::zf1_store(buf, ztw, v, r, j2);
     }
-    __syncthreads();
+    if (STAGED) __syncthreads();  // every row of the stage is read
+    else __syncwarp();
     if (STAGED && warp == 0 && next < N) {
       fence_proxy_async();
       issue(next);
@@ -784,12 +798,12 @@ __global__ void __launch_bounds__(kThreads, 2) plane_inv_fwd_kernel(const __grid
         reinterpret_cast<T2 *>(phi + rowoff)[j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
       });
     } else {
-      // phi rows [r][M] in buf
+      // phi rows [r][M] in buf (each warp writes and then reads its own rows)
       P::template zi2<true>(buf, tid, [&](int r, int j, T2 z) {
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
         buf[r * M + j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
       });
-      __syncthreads();
+      __syncwarp();
       {
         const int j2 = tid & 7, r = tid >> 3;
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
@@ -799,10 +813,10 @@ __global__ void __launch_bounds__(kThreads, 2) plane_inv_fwd_kernel(const __grid
           const int j = j1 * 8 + j2;
           v[j1] = Pro::pro(p, b, rowoff + 2 * j, buf[r * M + j], acc_p);
         });
-        __syncthreads();  // every row is read before the z exchange overwrites it
+        __syncwarp();  // the warp's rows are read before its z exchange overwrites them
         P::zf1_store(buf, ztw, v, r, j2);
       }
-      __syncthreads();
+      __syncwarp();
       P::zf2_post(buf, tw, tid, cluster);
       P::yf(buf, tw, tid, rank, cluster, dst, plane);
     }
