@@ -82,13 +82,22 @@ size_t spm_spectrum_bytes(const spm_ctx *ctx);
 const char *spm_status_str(int status);
 /* Tuning knobs (no counterpart in the reference; the analogue of FFTW's plan
  * choice, My_FFT.cpp:49-97). knob "plane_cps": 1 = plane kernels stage their
- * input in shared memory (one CTA per SM), 2 = direct loads, two CTAs per SM.
+ * input in shared memory (one CTA per SM), 2 = direct loads, two CTAs per SM,
+ * 3 = direct loads, three CTAs per SM (fewer registers per thread).
  * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
  * inverse plane pass with the next step's forward one (phi stays on chip
  * between steps; the same bits as 0), 0 = three passes per step.
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);
+/* Autotuner (no counterpart in the reference): times chains of `steps`
+ * gradient steps on a scratch field for each candidate schedule (plane_cps
+ * 1/2/3 with fused chains, plane_cps 2 without) and keeps the fastest in the
+ * context; the choice is remembered per (device, N, precision), so later
+ * contexts of the same kind take it without timing (FP32 twins of mixed flows
+ * included). Synchronises; allocates two scratch fields while it runs. The
+ * chosen knobs are returned in *plane_cps, *fuse_planes (may be NULL). */
+int spm_autotune(spm_ctx *ctx, int steps, int *plane_cps, int *fuse_planes);
 const char *spm_last_error(void);
 /* Number of transform-kernel launches issued by this context so far. */
 uint64_t spm_launch_count(const spm_ctx *ctx);

@@ -1,0 +1,114 @@
+// Autotuner for the transform schedule of a context (no counterpart in the
+// reference; FFTW's plan search plays this role there, My_FFT.cpp:49-97).
+// Candidates: the plane-pass variant (staged with one CTA per SM, direct loads
+// with two CTAs per SM, or three CTAs per SM with fewer registers per thread)
+// and whether gradient chains use the fused inverse -> forward plane pass.
+// Each candidate runs a short chain of gradient steps on a scratch field with
+// CUDA events around it; the fastest is kept in the context and remembered per
+// (device, N, precision) for later contexts.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "../../include/spmiqc.h"
+#include "spm_internal.h"
+
+namespace {
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_best;  // (device, N, prec) -> (plane_cps, fuse)
+
+// A smooth non-trivial field (a few cosines), so the timed steps do real work
+// and the flow does not stop on its first step.
+template <class T> __global__ void fill_kernel(T *phi, int N) {
+  const size_t n = (size_t)N * N * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i / ((size_t)N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    phi[i] = (T)(0.1 * (cospi(2.0 * (3 * x + 5 * y) / N) + sinpi(2.0 * (7 * z - 2 * x) / N)) +
+                 1e-3 * ((x * 31 + y * 17 + z * 13) % 29) / 29.0);
+  }
+}
+
+}  // namespace
+
+// The remembered choice for (device, N, precision), if any.
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_best.find(std::make_tuple(device, N, prec));
+  if (it == g_best.end()) return false;
+  *plane_cps = it->second.first;
+  *fuse_planes = it->second.second;
+  return true;
+}
+
+extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_planes) {
+  if (!c || steps < 2) return spm_fail(SPM_ERR_ARG, "bad argument (steps >= 2)");
+  const auto key = std::make_tuple(c->device, c->N, c->prec);
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_best.find(key);
+    if (it != g_best.end()) {
+      c->plane_cps = it->second.first;
+      c->fuse_planes = it->second.second;
+      if (plane_cps) *plane_cps = c->plane_cps;
+      if (fuse_planes) *fuse_planes = c->fuse_planes;
+      return SPM_OK;
+    }
+  }
+  void *phi = nullptr, *uh = nullptr;
+  cudaError_t e = cudaMalloc(&phi, c->field_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&uh, c->field_bytes);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int rc = e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "autotune buffers");
+  const int saved_cps = c->plane_cps, saved_fuse = c->fuse_planes;
+  int best_cps = saved_cps, best_fuse = saved_fuse;
+  float best = 1e30f;
+  const int cands[][2] = {{2, 1}, {3, 1}, {1, 1}, {2, 0}};
+  for (const auto &cand : cands) {
+    if (rc != SPM_OK) break;
+    c->plane_cps = cand[0];
+    c->fuse_planes = cand[1];
+    if (c->prec == SPM_FP64) fill_kernel<double><<<592, 256, 0, c->stream>>>((double *)phi, c->N);
+    else fill_kernel<float><<<592, 256, 0, c->stream>>>((float *)phi, c->N);
+    rc = spm_fft(c, phi, uh);
+    // warm-up (kernel attributes, occupancy queries, caches), then the best of three timed chains
+    if (rc == SPM_OK) rc = spm_grad_flow_enqueue(c, phi, uh, 3, 0.0);
+    if (rc == SPM_OK) rc = spm_grad_flow_collect(c, nullptr, 0, nullptr);
+    float t = 1e30f;
+    for (int r = 0; r < 3 && rc == SPM_OK; r++) {
+      cudaEventRecord(e0, c->stream);
+      rc = spm_grad_flow_enqueue(c, phi, uh, steps, 0.0);
+      cudaEventRecord(e1, c->stream);
+      if (rc == SPM_OK) rc = spm_grad_flow_collect(c, nullptr, 0, nullptr);
+      float ms = 0;
+      if (rc == SPM_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < t) t = ms;
+    }
+    if (rc == SPM_OK && t < best) {
+      best = t;
+      best_cps = cand[0];
+      best_fuse = cand[1];
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(phi);
+  cudaFree(uh);
+  if (rc != SPM_OK) {
+    c->plane_cps = saved_cps;
+    c->fuse_planes = saved_fuse;
+    return rc;
+  }
+  c->plane_cps = best_cps;
+  c->fuse_planes = best_fuse;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_best[key] = {best_cps, best_fuse};
+  }
+  if (plane_cps) *plane_cps = best_cps;
+  if (fuse_planes) *fuse_planes = best_fuse;
+  return SPM_OK;
+}

@@ -751,9 +751,10 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
 // flow stops (the pencil pass armed FW_PENDING): the forward half is then
 // skipped. A chain of K steps is plane_fwd, K pencils, K-1 of these and one
 // plane_inv, so the real field crosses HBM once per chain instead of twice per
-// step. Direct loads, two CTAs per SM (the CPS = 2 layout).
-template <int N, class T, class Epi, class Pro>
-__global__ void __launch_bounds__(kThreads, 2) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
+// step. Direct loads; CPS (2 or 3) CTAs per SM, the layout of plane_fwd's
+// direct variant.
+template <int N, class T, class Epi, class Pro, int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
   using P = Plane<N, T>;

@@ -68,6 +68,10 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
 // The plane kernels come in two variants (c->plane_cps): 1 = staged, one CTA
 // per SM; 2 = direct loads, two CTAs per SM.
 template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
+  if (c->plane_cps == 3) {
+    struct Tag3 {};
+    return launch_cluster<Tag3, N>(c, plane_fwd_kernel<N, T, Pro, 3>, plane_smem<N, T, 3>(), p, nb, "plane_fwd");
+  }
   if (c->plane_cps == 2) {
     struct Tag2 {};
     return launch_cluster<Tag2, N>(c, plane_fwd_kernel<N, T, Pro, 2>, plane_smem<N, T, 2>(), p, nb, "plane_fwd");
@@ -76,6 +80,10 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
   return launch_cluster<Tag1, N>(c, plane_fwd_kernel<N, T, Pro, 1>, plane_smem<N, T, 1>(), p, nb, "plane_fwd");
 }
 template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p0, int nb) {
+  if (c->plane_cps == 3) {
+    struct Tag3 {};
+    return launch_cluster<Tag3, N>(c, plane_inv_kernel<N, T, Epi, 3>, plane_smem<N, T, 3>(), p0, nb, "plane_inv");
+  }
   if (c->plane_cps == 2) {
     struct Tag2 {};
     return launch_cluster<Tag2, N>(c, plane_inv_kernel<N, T, Epi, 2>, plane_smem<N, T, 2>(), p0, nb, "plane_inv");
@@ -85,11 +93,17 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
   for (int b = 0; b < nb; b++) SPM_TRY(spm_tensor_map(c, p.in[b], TM_PLANE_INV, &p.tmi[b]));
   return launch_cluster<Tag1, N>(c, plane_inv_kernel<N, T, Epi, 1>, plane_smem<N, T, 1>(), p, nb, "plane_inv");
 }
-// The fused inverse -> forward plane pass (direct loads, two CTAs per SM).
+// The fused inverse -> forward plane pass (direct loads; two CTAs per SM, or
+// three with plane_cps = 3).
 template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
-  struct Tag {};
-  return launch_cluster<Tag, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro>, plane_smem<N, T, 2>(), p, nb,
-                                "plane_inv_fwd");
+  if (c->plane_cps == 3) {
+    struct Tag3 {};
+    return launch_cluster<Tag3, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 3>, plane_smem<N, T, 3>(), p, nb,
+                                   "plane_inv_fwd");
+  }
+  struct Tag2 {};
+  return launch_cluster<Tag2, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 2>, plane_smem<N, T, 2>(), p, nb,
+                                 "plane_inv_fwd");
 }
 // Persistent pencil launch: resident CTAs (queried once), at most one per tile.
 template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p0, int nb) {

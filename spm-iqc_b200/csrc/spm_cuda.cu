@@ -303,7 +303,7 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
 extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
   if (!c || !knob) return spm_fail(SPM_ERR_ARG, "null argument");
   if (std::strcmp(knob, "plane_cps") == 0) {
-    if (value != 1 && value != 2) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1 or 2");
+    if (value < 1 || value > 3) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1, 2 or 3");
     c->plane_cps = value;
     return SPM_OK;
   }
@@ -488,6 +488,8 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->cancel = c->cancel;
   c->twin->plane_cps = c->plane_cps;
   c->twin->fuse_planes = c->fuse_planes;
+  // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
+  spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes);
   return SPM_OK;
 }
 

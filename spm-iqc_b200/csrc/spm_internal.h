@@ -73,4 +73,6 @@ void spm_free_extra(spm_ctx *c);
 // Creates (once) the FP32 twin context and its two FP32 fields, and binds it
 // to the context's stream, cancel flag and tuning.
 int spm_ensure_twin(spm_ctx *c);
+// The autotuner's remembered choice for (device, N, precision), if any.
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes);
 const struct OpsTable *spm_table_of(const spm_ctx *c);

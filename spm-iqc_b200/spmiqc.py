@@ -235,6 +235,14 @@ class SpmContext:
         f.argtypes = [_vp, ctypes.c_char_p, ctypes.c_int]
         check(f(self.h, knob.encode(), int(value)))
 
+    def autotune(self, steps: int = 20):
+        """spm_autotune: times the candidate schedules, keeps the fastest; returns (plane_cps, fuse_planes)."""
+        f = lib().spm_autotune
+        f.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(f(self.h, int(steps), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def ngrad_cam(self, phi, grad=None):
         grad = self.field() if grad is None else grad
         nrm = ctypes.c_double()

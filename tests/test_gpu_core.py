@@ -132,3 +132,29 @@ def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
     assert len(b0) < 3000 and len(b0) == len(b1)
     assert np.array_equal(a0, a1) and np.array_equal(b0, b1)
     assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
+
+
+def test_autotune_picks_a_schedule_and_keeps_results(spm, cuda):
+    """The autotuner returns one of its candidates, remembers it for the next
+    context of the same kind, and every schedule gives the same fields (the
+    transforms' arithmetic does not depend on the schedule) with records equal
+    to rounding (the reduction grids differ)."""
+    N = 64
+    c = spm.SpmContext(N)
+    cps, fuse = c.autotune(10)
+    assert cps in (1, 2, 3) and fuse in (0, 1)
+    d = spm.SpmContext(N)
+    assert d.autotune(10) == (cps, fuse)
+    phi = npo.uniform_field(N, 8)
+    out = []
+    for k_cps, k_fuse in ((1, 1), (2, 1), (3, 1), (2, 0)):
+        e = spm.SpmContext(N)
+        e.tune("plane_cps", k_cps)
+        e.tune("fuse_planes", k_fuse)
+        p = t(cuda, phi)
+        u = e.my_fft(p)
+        st = e.get_min_u_F(p, u, 20)
+        out.append((st, p.cpu().numpy()))
+    for st, p in out[1:]:
+        assert np.array_equal(p, out[0][1])
+        assert rel(st, out[0][0]) < 1e-13
