@@ -287,6 +287,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
                : "memory");
 }
 // dst/src 16-byte aligned, bytes a multiple of 16.
+// Asks for `bytes` at src (16-byte aligned, a multiple of 16) to be brought
+// into L2; no registers, shared memory or completion tracking involved.
+__device__ __forceinline__ void prefetch_l2(const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+// Cluster barrier halves. arrive_relaxed orders nothing: use it where a CTA
+// only signals that it has finished READING other CTAs' shared memory (every
+// loaded value already consumed by an instruction before it), so that they
+// may overwrite it after their wait.
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(

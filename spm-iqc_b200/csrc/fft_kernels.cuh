@@ -168,8 +168,10 @@ template <int N, class T> struct Plane {
         const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
         v[j1] = rem[(y & 31) * M + col];
       });
-      cluster.sync();
-      Dft<-1, M1, T2>::run(v);
+      Dft<-1, M1, T2>::run(v);  // consumes every gathered value
+      // done reading the other CTAs' rows: they may overwrite them after the wait
+      cluster_arrive_relaxed();
+      cluster_wait();
       sfor<0, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
         buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmul(v[k1], tw[j2 * k1]);
@@ -263,7 +265,9 @@ template <int N, class T> struct Plane {
         zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
       }
     }
-    cluster.sync();
+    // every gathered value is consumed: done reading the column owners
+    cluster_arrive_relaxed();
+    cluster_wait();
 #pragma unroll
     for (int i = 0; i < TPT; i++) {
       const int task = lane + 32 * i;
@@ -403,6 +407,9 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
   for (int it = 0; plane < N; plane += ncl, it++) {
     const int next = plane + ncl;
     if (STAGED) mbar_wait(bar, it & 1, &s_err);
+    // next plane's rows towards L2 while this one is transformed
+    if (!STAGED && next < N && tid < kRows)
+      prefetch_l2(src + ((size_t)next * N + rank * kRows + tid) * N, N * sizeof(T));
     {
       const int j2 = tid & 7, r = tid >> 3;
       const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
@@ -718,6 +725,9 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   for (int it = 0; plane < N; plane += ncl, it++) {
     const int next = plane + ncl;
     if (STAGED) mbar_wait(bar, it & 1, &s_err);
+    // next plane's columns towards L2 while this one is transformed
+    if (!STAGED && next < N && tid < N)
+      prefetch_l2(gsrc + ((size_t)next * N + tid) * M + rank * kCols, kCols * sizeof(T2));
     P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
       return STAGED ? stage[ky * 16 + c] : __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
     });
@@ -788,6 +798,9 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
   T *phi = reinterpret_cast<T *>(p.sto[b]);
 
   for (int plane = cid; plane < N; plane += ncl) {
+    // next plane's columns towards L2 while this one is transformed
+    if (plane + ncl < N && tid < N)
+      prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + tid) * M + rank * kCols, kCols * sizeof(T2));
     P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
       return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
     });
