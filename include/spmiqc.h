@@ -226,6 +226,15 @@ int spm_spring_pairing(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double
 int spm_spring_pairing_mixed(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double switch_tol,
                              double *res_hist, int *iters_fp32, int *iters_fp64);
 
+/* hiosd_lobpcg_sieh (HISD.cpp:86-485): k-index saddle dynamics from x along
+ * the k directions V (k fields, 1 <= k <= 8), both updated in place, with the
+ * reference's options dt, betat, betau (Barzilai-Borwein step clamp), epsf
+ * (stop when ||grad F|| < epsf) and maxiter (critical_point_HISD,
+ * HISD.cpp:13-31, uses 0.8, 8.0, 0.02, 1e-7, 10000). res_hist (host, may be
+ * NULL, >= maxiter entries) receives ||grad F|| per iteration. */
+int spm_hisd(spm_ctx *ctx, void *x, void *V, int k, double dt, double betat, double betau, double epsf,
+             int maxiter, double *res_hist, int *iters);
+
 /* ------------------------------------------------------------ BLAS-1 */
 
 /* inpfp (BasicOperators.cpp:132-143): <p, q> = (1/N^3) sum p q. */

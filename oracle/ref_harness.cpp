@@ -23,6 +23,7 @@
 #include "BasicOperators.h"
 #include "Data.h"
 #include "File_Op.h"
+#include "HISD.h"
 #include "Initialization.h"
 #include "LOBPCG.h"
 #include "LPsrc.h"
@@ -328,6 +329,34 @@ void ref_spring_pairing(double *phi0, double *phi1, double maxiter, double tol) 
   }
   to_real(Phi0[0], phi0);
   to_real(Phi0[1], phi1);
+}
+
+// HISD.cpp:86-485 on (x, V) in place with the given options.
+void ref_hisd(double *xr, int k, double *V, double dt, double betat, double betau, double epsf, int maxiter) {
+  if (!g_opt || g_opt->k != k) {
+    free_option();
+    spm_shim_eigen_seed(0);
+    g_opt = (Option *)malloc(sizeof(Option));
+    Mute m;
+    hiosd_lobpcg_initialization(g_opt, k);
+  }
+  for (int i = 0; i < k; i++) to_cplx(V + (size_t)i * CplxDofs_local, g_opt->V[i]);
+  g_opt->dt = dt;
+  g_opt->betat = betat;
+  g_opt->betau = betau;
+  g_opt->epsf = epsf;
+  g_opt->maxiter = maxiter;
+  g_opt->outputp = 100;
+  g_opt->outputd = 1000;
+  fftw_complex *x = alloc_c();
+  to_cplx(xr, x);
+  {
+    Mute m;
+    hiosd_lobpcg_sieh(x, g_opt);
+  }
+  to_real(x, xr);
+  for (int i = 0; i < k; i++) to_real(g_opt->V[i], V + (size_t)i * CplxDofs_local);
+  free(x);
 }
 
 // File_Op.cpp:40-61 (Save_phi / load_phi) on a real field.

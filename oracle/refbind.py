@@ -66,6 +66,7 @@ def lib(path: str = LIB):
         L.ref_save_option_v.argtypes = [ctypes.c_int, _dp, ctypes.c_char_p]
         L.ref_load_option_v.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
         L.ref_initial_value.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
+        L.ref_hisd.argtypes = [_dp, ctypes.c_int, _dp] + [ctypes.c_double] * 4 + [ctypes.c_int]
         _libs[path] = L
     return _libs[path]
 
@@ -169,6 +170,13 @@ class Ref:
         b = np.array(phi1, dtype=np.float64, order="C")
         self.L.ref_spring_pairing(_p(a), _p(b), float(maxiter), float(tol))
         return a, b
+
+    def hisd(self, x, V, dt=0.8, betat=8.0, betau=0.02, epsf=1e-7, maxiter=10000):
+        """hiosd_lobpcg_sieh on copies of (x, V); returns the updated pair."""
+        x = np.array(x, dtype=np.float64, order="C")
+        V = np.array(V, dtype=np.float64, order="C")
+        self.L.ref_hisd(_p(x), V.shape[0], _p(V), dt, betat, betau, epsf, int(maxiter))
+        return x, V
 
     # File_Op.cpp: the reference's field files
     def save_phi(self, phi, path):

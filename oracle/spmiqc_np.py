@@ -232,6 +232,93 @@ class Model:
                 V[i] *= 1.0 / self.nrmp(V[i])
         return V, ritz
 
+    def _lob_step(self, x, V, U, W, Y, Vp, Up):
+        """One iteration body of src/HISD.cpp:258-444 (the LOBPCG update of V
+        at position x, with the previous V as the P block); returns the new V."""
+        k = V.shape[0]
+        shape = V.shape
+        emp = np.ones(3 * k, dtype=bool)
+        for i in range(k):
+            U[i] = self.hv(x, V[i])
+            a = self.inpfp(V[i], U[i])
+            W[i] = 1 * U[i] + (-a) * V[i]
+            W[i] = self.precond(W[i])
+            self.orth_v2V(W[i], V, k)
+            self.orth_Vi(W, i)
+            nw = self.nrmp(W[i])
+            if nw > 1e-8:
+                W[i] *= 1.0 / nw
+                Y[i] = self.hv(x, W[i])
+            else:
+                W[i] = 0.0
+                Y[i] = 0.0
+                emp[k + i] = False
+        for i in range(k):
+            self.orth_v2V(Vp[i], V, k)
+            self.orth_v2V(Vp[i], W, k)
+            self.orth_Vi(Vp, i)
+            nv = self.nrmp(Vp[i])
+            if nv > 1e-8:
+                Vp[i] *= 1.0 / nv
+                Up[i] = self.hv(x, Vp[i])
+            else:
+                Vp[i] = 0.0
+                Up[i] = 0.0
+                emp[2 * k + i] = False
+        UU = np.concatenate([V, W, Vp]).reshape(3 * k, -1)[emp]
+        YY = np.concatenate([U, Y, Up]).reshape(3 * k, -1)[emp]
+        P = UU @ YY.T
+        P = (P.T + P) * 0.5 / self.n3
+        vals, vecs = np.linalg.eigh(P)
+        Vp[:] = V
+        Up[:] = U
+        V = (vecs[:, :k].T @ UU).reshape(shape)
+        for i in range(k):
+            V[i] -= np.sum(V[i]) / self.n3
+        for i in range(k):
+            self.orth_v2V(V[i], V, i)
+            V[i] *= 1.0 / self.nrmp(V[i])
+        return V
+
+    # src/HISD.cpp:86-485 (hiosd_lobpcg_sieh)
+    def hisd(self, x, V, dt=0.8, betat=8.0, betau=0.02, epsf=1e-7, maxiter=10000):
+        """Returns (x, V, residual history)."""
+        k = V.shape[0]
+        x = x.copy()
+        V = V.copy()
+        shape = V.shape
+        U, W, Y, Vp, Up = (np.zeros(shape) for _ in range(5))
+        for i in range(k):
+            self.orth_Vi(V, i)
+            V[i] *= 1.0 / self.nrmp(V[i])
+        pv = lambda f: sum(self.inpfp(f, V[i]) * V[i] for i in range(k))  # PV_Cplx
+        f = self.ngrad(x)
+        gp = np.zeros_like(x)
+        Dx = f - 2.0 * pv(f) + dt  # FuncRealAddAConst (HISD.cpp:180)
+        hist = []
+        for _ in range(maxiter):
+            tm = 2.0 * pv(f)
+            g = f - tm
+            Dg = g - gp
+            gp = g
+            bta = abs(self.inpfp(Dx, Dg) / self.inpfp(Dg, Dg))
+            bta = max(min(bta, betat * dt), betau * dt)
+            xp = x
+            nln = self.Tau * x + self.Gamma * x * x - x * x * x
+            nln = nln - np.sum(nln) / self.n3
+            rho = (self.my_fft(x) + bta * self.my_fft(nln) - bta * self.my_fft(tm)) / (1 + bta * self.G)
+            rho = rho.real + 0j          # the reference keeps the real part only (HISD.cpp:249-252)
+            rho[0, 0, 0] = 0.0
+            x = self.my_ifft(rho).real
+            Dx = x - xp
+            V = self._lob_step(x, V, U, W, Y, Vp, Up)
+            f = self.ngrad(x)
+            res = self.nrmp(f)
+            hist.append(res)
+            if res < epsf:
+                break
+        return x, V, np.array(hist)
+
     def rayleigh(self, x, v) -> float:
         """src/BasicOperators.cpp:174-185."""
         return self.inpfp(v, self.hv(x, v)) / self.inpfp(v, v)

@@ -140,6 +140,20 @@ template <class T> struct ProTangent {
   }
 };
 
+// HiSD position step (HISD.cpp:200-256): transforms y = x + beta (N(x) - T)
+// with N = Tau x + Gamma x^2 - x^3 (its mean only reaches the k = 0 mode,
+// which the step zeroes) and T = 2 PV(f) (aux0); beta in m.factor.
+template <class T> struct ProHisd {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&)[1]) {
+    const c2<T> t = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma, beta = (T)p.m.factor;
+    return c2<T>{x.x + beta * (poly_force(x.x, tau, gam) - t.x), x.y + beta * (poly_force(x.y, tau, gam) - t.y)};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
 // ===================================================================== pencil ops
 // Forward transform with the reference's 1/N^3 (My_FFT.cpp:9-13): store only.
 template <class T> struct OpFwd {
@@ -287,6 +301,23 @@ template <class T, bool NORM = true> struct OpTangent {
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}
 };
 
+// HiSD spectral update (HISD.cpp:246-256): x'^ = Re(y^ / (1 + beta G)) with
+// the imaginary part set to 0, as the reference does, and x'^_0 = 0.
+template <class T> struct OpHisd {
+  static constexpr bool FI = true, SI = false, SO = false, INV = true, LIN = false;
+  static constexpr int SYM = 0;
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T>, c2<T> &,
+                               c2<T> &inv, double (&)[1], double) {
+    const T beta = (T)p.m.factor;
+    const T den = (T)1 + beta * (T)sy.x;
+    inv = c2<T>{f.x * (T)p.m.inv_n3 / den, (T)0};
+    if (Kx == 0 && Ky == 0 && Kz == 0) inv = c2<T>{0, 0};
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
 // E1 = 1/2 sum_k G |u_k|^2 of a stored spectrum (LPsrc.cpp:27-35): reduction only.
 template <class T> struct OpE1 {
   static constexpr bool FI = false, SI = true, SO = false, INV = false, LIN = false;
@@ -371,6 +402,19 @@ template <class T> struct EpiTangent {
       const T d = (T)sqrt(scal_of(p, b)[SC_NRM2]);
       *reinterpret_cast<c2<T> *>(reinterpret_cast<T *>(p.sto[b]) + idx) = c2<T>{(c.x - a.x) / d, (c.y - a.y) / d};
     }
+    return y;
+  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
+};
+
+// HiSD epilogue: stores x' and Dx = x' - x (p.sto) where x is the field being
+// overwritten (p.aux1; each value is read by the thread that writes it).
+template <class T> struct EpiHisd {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&)[1]) {
+    const c2<T> x = *reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx);
+    *reinterpret_cast<c2<T> *>(reinterpret_cast<T *>(p.sto[b]) + idx) = c2<T>{y.x - x.x, y.y - x.y};
     return y;
   }
   __device__ static void fin(const KParams &, int, const double (&)[1]) {}

@@ -5,6 +5,7 @@
 
 #include <atomic>
 
+#include "../../include/spmiqc.h"
 #include "blas1.cuh"
 #include "spm_internal.h"
 #include "spm_table.h"
@@ -145,8 +146,18 @@ template <int N, class T, class F> static int reduce(spm_ctx *c, const KParams &
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, "reduce launch");
 }
 
+// Every chain that goes through the spectral scratch checks that the caller
+// made room for its batch (spm_ensure_scratch) instead of writing through an
+// unallocated buffer.
+#define SPM_NEED_SCRATCH(c, nb)                                                         \
+  do {                                                                                  \
+    if ((c)->scratch_cap < (nb) || !(c)->bufA || !(c)->bufB)                            \
+      return spm_fail(SPM_ERR_STATE, "spectral scratch not allocated for this batch"); \
+  } while (0)
+
 template <int N, class T> struct Impl {
   static int fft(spm_ctx *c, const void *x, void *xhat) {
+    SPM_NEED_SCRATCH(c, 1);
     KParams p = spm_params(c);
     p.in[0] = x;
     p.out[0] = spm_bufA(c, 0);
@@ -158,6 +169,7 @@ template <int N, class T> struct Impl {
   }
 
   static int ifft(spm_ctx *c, const void *xhat, void *x) {
+    SPM_NEED_SCRATCH(c, 1);
     KParams q = spm_params(c);
     q.st[0] = xhat;
     q.out[0] = spm_bufB(c, 0);
@@ -181,6 +193,7 @@ template <int N, class T> struct Impl {
   // One fused semi-implicit step, gated by the flow words. With ev non-null,
   // records ev[0..3] around the three passes (for per-kernel timing).
   static int grad_step_ev(spm_ctx *c, void *phi, void *uhat, void *const *ev) {
+    SPM_NEED_SCRATCH(c, 1);
     auto rec = [&](int i) {
       if (ev) cudaEventRecord((cudaEvent_t)ev[i], c->stream);
     };
@@ -219,6 +232,7 @@ template <int N, class T> struct Impl {
   // ev[1] after it and ev[2 + 2k], ev[3 + 2k] after step k's pencil and plane
   // pass (for per-kernel timing).
   static int grad_steps_ev(spm_ctx *c, void *phi, void *uhat, int K, void *const *ev) {
+    SPM_NEED_SCRATCH(c, 1);
     if (K <= 0) return 0;
     auto rec = [&](int i) {
       if (ev) cudaEventRecord((cudaEvent_t)ev[i], c->stream);
@@ -265,6 +279,7 @@ template <int N, class T> struct Impl {
 
   // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
   static int ngrad(spm_ctx *c, const void *phi, void *grad) {
+    SPM_NEED_SCRATCH(c, 1);
     KParams p = spm_params(c);
     p.in[0] = phi;
     p.out[0] = spm_bufA(c, 0);
@@ -282,6 +297,7 @@ template <int N, class T> struct Impl {
 
   // n <= kMaxBatch Hessian-vector products sharing phi.
   static int hv(spm_ctx *c, const void *phi, const void *const *v, void *const *hv, int n) {
+    SPM_NEED_SCRATCH(c, n);
     KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
     for (int b = 0; b < n; b++) {
       p.in[b] = v[b];
@@ -301,6 +317,7 @@ template <int N, class T> struct Impl {
 
   // n <= kMaxBatch preconditioner applications, in place.
   static int precond(spm_ctx *c, void *const *w, int n) {
+    SPM_NEED_SCRATCH(c, n);
     KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
     for (int b = 0; b < n; b++) {
       p.in[b] = w[b];
@@ -328,6 +345,7 @@ template <int N, class T> struct Impl {
   // written to v_out; with phi0 null, phi1 is the tangent as given. Always
   // writes vhat = FFT(v)/N^3 (packed) and Gv = IFFT(G vhat, k = 0 removed).
   static int tangent(spm_ctx *c, const void *phi0, const void *phi1, void *v_out, void *vhat, void *gv) {
+    SPM_NEED_SCRATCH(c, 1);
     KParams p = spm_params(c);
     p.in[0] = phi1;
     p.aux0[0] = phi0;
@@ -352,6 +370,7 @@ template <int N, class T> struct Impl {
   // all along the tangent (v, vhat, Gv) from tangent().
   static int force(spm_ctx *c, void *const *x, int n, const void *v, const void *vhat, const void *gv,
                    double factor) {
+    SPM_NEED_SCRATCH(c, n);
     KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
     p.m.factor = factor;
     for (int b = 0; b < n; b++) {
@@ -370,8 +389,31 @@ template <int N, class T> struct Impl {
     return plane_inv<N, T, EpiStore<T>>(c, r, n);
   }
 
+  // HiSD position step: x <- IFFT(Re(FFT(x + beta (N(x) - t)) / N^3 / (1 + beta G))), dx = x' - x.
+  static int hisd_step(spm_ctx *c, void *x, const void *t, void *dx, double beta) {
+    SPM_NEED_SCRATCH(c, 1);
+    KParams p = spm_params(c);
+    p.m.factor = beta;
+    p.in[0] = x;
+    p.aux0[0] = t;
+    p.out[0] = spm_bufA(c, 0);
+    SPM_TRY((plane_fwd<N, T, ProHisd<T>>(c, p, 1)));
+    KParams q = spm_params(c);
+    q.m.factor = beta;
+    q.in[0] = spm_bufA(c, 0);
+    q.out[0] = spm_bufB(c, 0);
+    SPM_TRY((pencil<N, T, OpHisd<T>>(c, q, 1)));
+    KParams r = spm_params(c);
+    r.in[0] = spm_bufB(c, 0);
+    r.aux1[0] = x;
+    r.sto[0] = dx;
+    r.out[0] = x;
+    return plane_inv<N, T, EpiHisd<T>>(c, r, 1);
+  }
+
   // ||ngrad(x_b)||^2 -> scal[b][SC_GN2] without storing the gradient.
   static int gnorm(spm_ctx *c, const void *const *x, int n) {
+    SPM_NEED_SCRATCH(c, n);
     KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
     for (int b = 0; b < n; b++) {
       p.in[b] = x[b];
@@ -389,7 +431,7 @@ template <int N, class T> struct Impl {
 
   static const OpsTable *table() {
     static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_steps_ev, &grad_step_ev, &ngrad, &hv, &precond, &dot,
-                               &tangent, &force, &gnorm};
+                               &tangent, &force, &gnorm, &hisd_step};
     return &t;
   }
 };

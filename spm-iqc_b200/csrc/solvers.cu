@@ -40,6 +40,7 @@ struct Solver {
   void *spm = nullptr;          // SPM: v, vhat, Gv
   double *spm_stats = nullptr;
   int spm_cap = 0;
+  void *hisd = nullptr;         // HiSD: f, 2 PV(f), g, gp, Dx, Dg
 };
 
 Solver *solver(spm_ctx *c) {
@@ -293,6 +294,11 @@ int orth_with_drop(spm_ctx *c, void *const *X, int k, double thr, std::vector<in
   return SPM_OK;
 }
 
+int zero_fields(spm_ctx *c, void *dst, int k) {
+  cudaError_t e = cudaMemsetAsync(dst, 0, c->field_bytes * (size_t)k, c->stream);
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "zero");
+}
+
 int copy_fields(spm_ctx *c, void *dst, const void *src, int k) {
   if (dst == src) return SPM_OK;
   cudaError_t e = cudaMemcpyAsync(dst, src, c->field_bytes * (size_t)k, cudaMemcpyDeviceToDevice, c->stream);
@@ -311,6 +317,7 @@ void spm_free_extra(spm_ctx *c) {
   cudaFree(s->lob);
   cudaFree(s->spm);
   cudaFree(s->spm_stats);
+  cudaFree(s->hisd);
   if (s->h_gram) cudaFreeHost(s->h_gram);
   delete s;
   c->extra = nullptr;
@@ -341,11 +348,13 @@ extern "C" int spm_lobpcg_init(spm_ctx *c, void *V, int k, uint64_t seed) {
   return orthonormalize(c, X.data(), k);
 }
 
-extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
-                          double *resid, int *iters) {
-  if (!c || !phi || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0)
-    return spm_fail(SPM_ERR_ARG, "bad argument (k must be in [1, 8])");
-  SPM_TRY(ensure_base(c));
+// The blocks of one LOBPCG run: V (current), U = H V, W (preconditioned
+// residuals), Y = H W, P (previous V), Up = H P, Vn (scratch for the new V).
+struct LobBlocks {
+  std::vector<void *> Vc, U, W, Y, P, Up, Vn;
+};
+
+static int lob_blocks(spm_ctx *c, void *V, int k, LobBlocks &B) {
   Solver *s = solver(c);
   if (s->lob_k < k) {
     cudaFree(s->lob);
@@ -355,106 +364,125 @@ extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxit
     if (e != cudaSuccess) return spm_fail_cuda(e, "LOBPCG work fields");
     s->lob_k = k;
   }
-  std::vector<void *> Vc(k), U(k), W(k), Y(k), P(k), Up(k), Vn(k);
+  B = LobBlocks{};
   for (int i = 0; i < k; i++) {
-    Vc[i] = fld(c, V, i);
-    U[i] = fld(c, s->lob, i);
-    W[i] = fld(c, s->lob, k + i);
-    Y[i] = fld(c, s->lob, 2 * k + i);
-    P[i] = fld(c, s->lob, 3 * k + i);
-    Up[i] = fld(c, s->lob, 4 * k + i);
-    Vn[i] = fld(c, s->lob, 5 * k + i);
+    B.Vc.push_back(fld(c, V, i));
+    B.U.push_back(fld(c, s->lob, i));
+    B.W.push_back(fld(c, s->lob, k + i));
+    B.Y.push_back(fld(c, s->lob, 2 * k + i));
+    B.P.push_back(fld(c, s->lob, 3 * k + i));
+    B.Up.push_back(fld(c, s->lob, 4 * k + i));
+    B.Vn.push_back(fld(c, s->lob, 5 * k + i));
   }
-  std::vector<double> G, T;
+  return SPM_OK;
+}
+
+// First half of an iteration (LOBPCG.cpp:270-286): U = H V, alpha = <V, U>,
+// W = U - alpha V and res_i = ||W_i||.
+static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::vector<double> &alpha,
+                        std::vector<double> &res) {
+  std::vector<double> G;
+  SPM_TRY(hv_many(c, phi, B.Vc.data(), B.U.data(), k));
+  SPM_TRY(gram(c, B.Vc.data(), k, B.U.data(), k, G));
+  for (int i = 0; i < k; i++) alpha[i] = G[(size_t)i * k + i];
+  {
+    std::vector<void *> X(2 * k);
+    std::vector<double> C((size_t)2 * k * k, 0.0);
+    for (int i = 0; i < k; i++) {
+      X[i] = B.U[i];
+      X[k + i] = B.Vc[i];
+      C[(size_t)i * k + i] = 1.0;
+      C[(size_t)(k + i) * k + i] = -alpha[i];
+    }
+    SPM_TRY(combine(c, X.data(), 2 * k, B.W.data(), k, C, nullptr, false));
+  }
+  SPM_TRY(gram(c, B.W.data(), k, B.W.data(), k, G));
+  for (int i = 0; i < k; i++) res[i] = std::sqrt(std::max(0.0, G[(size_t)i * k + i]));
+  return SPM_OK;
+}
+
+// Second half (LOBPCG.cpp:287-449): W = P0(precond(W)) perp V with
+// Gram-Schmidt and the 1e-8 dropping, Y = H W; P perp [V, W], dropping,
+// Up = H P; Rayleigh-Ritz on [V; W; P]; P <- V; V <- the k lowest Ritz
+// vectors, mean removed and Gram-Schmidt orthonormalised.
+static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &have_p) {
+  std::vector<double> G;
+  SPM_TRY(precond_many(c, B.W.data(), k));
+  SPM_TRY(project_out(c, B.Vc.data(), k, B.W.data(), k));
+  std::vector<int> keepW(k, 1), keepP(k, 0);
+  SPM_TRY(orth_with_drop(c, B.W.data(), k, 1e-8, keepW));
+  SPM_TRY(hv_many(c, phi, B.W.data(), B.Y.data(), k));
+  if (have_p) {
+    std::vector<void *> VW(2 * k);
+    for (int i = 0; i < k; i++) {
+      VW[i] = B.Vc[i];
+      VW[k + i] = B.W[i];
+    }
+    SPM_TRY(project_out(c, VW.data(), 2 * k, B.P.data(), k));
+    keepP.assign(k, 1);
+    SPM_TRY(orth_with_drop(c, B.P.data(), k, 1e-8, keepP));
+    SPM_TRY(hv_many(c, phi, B.P.data(), B.Up.data(), k));
+  }
+  std::vector<void *> S, HS;
+  for (int i = 0; i < k; i++) {
+    S.push_back(B.Vc[i]);
+    HS.push_back(B.U[i]);
+  }
+  for (int i = 0; i < k; i++)
+    if (keepW[i]) {
+      S.push_back(B.W[i]);
+      HS.push_back(B.Y[i]);
+    }
+  for (int i = 0; i < k; i++)
+    if (keepP[i]) {
+      S.push_back(B.P[i]);
+      HS.push_back(B.Up[i]);
+    }
+  const int m = (int)S.size();
+  SPM_TRY(gram(c, S.data(), m, HS.data(), m, G));
+  std::vector<double> Gs((size_t)m * m), vals, vecs;
+  for (int i = 0; i < m; i++)
+    for (int j = 0; j < m; j++) Gs[(size_t)i * m + j] = (G[(size_t)j * m + i] + G[(size_t)i * m + j]) * 0.5;
+  sym_eig(Gs, m, vals, vecs);
+  std::vector<double> C((size_t)m * k);
+  for (int p = 0; p < m; p++)
+    for (int q = 0; q < k; q++) C[(size_t)p * k + q] = vecs[(size_t)p * m + q];
+  SPM_TRY(combine(c, S.data(), m, B.Vn.data(), k, C, nullptr, false));
+  std::swap(B.P, B.Vc);   // P holds the old V
+  std::swap(B.Vc, B.Vn);  // V holds the new block
+  have_p = true;
+  std::vector<double> mu;
+  SPM_TRY(means(c, B.Vc.data(), k, mu));
+  std::vector<double> I((size_t)k * k, 0.0), d(k);
+  for (int i = 0; i < k; i++) {
+    I[(size_t)i * k + i] = 1.0;
+    d[i] = -mu[i];
+  }
+  SPM_TRY(combine(c, B.Vc.data(), k, B.Vc.data(), k, I, &d, false));
+  return orthonormalize(c, B.Vc.data(), k);
+}
+
+extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
+                          double *resid, int *iters) {
+  if (!c || !phi || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0)
+    return spm_fail(SPM_ERR_ARG, "bad argument (k must be in [1, 8])");
+  SPM_TRY(ensure_base(c));
+  LobBlocks B;
+  SPM_TRY(lob_blocks(c, V, k, B));
   std::vector<double> alpha(k, 0.0), res(k, 0.0);
-  SPM_TRY(orthonormalize(c, Vc.data(), k));  // LOBPCG.cpp:262-267
+  SPM_TRY(orthonormalize(c, B.Vc.data(), k));  // LOBPCG.cpp:262-267
   int it = 0;
   bool have_p = false;
   for (;; it++) {
-    // U = H V, alpha = <V, U>, W = U - alpha V and its norm (the residual)
-    SPM_TRY(hv_many(c, phi, Vc.data(), U.data(), k));
-    SPM_TRY(gram(c, Vc.data(), k, U.data(), k, G));
-    for (int i = 0; i < k; i++) alpha[i] = G[(size_t)i * k + i];
-    {
-      std::vector<void *> X(2 * k);
-      std::vector<double> C((size_t)2 * k * k, 0.0);
-      for (int i = 0; i < k; i++) {
-        X[i] = U[i];
-        X[k + i] = Vc[i];
-        C[(size_t)i * k + i] = 1.0;
-        C[(size_t)(k + i) * k + i] = -alpha[i];
-      }
-      SPM_TRY(combine(c, X.data(), 2 * k, W.data(), k, C, nullptr, false));
-    }
-    SPM_TRY(gram(c, W.data(), k, W.data(), k, G));
+    SPM_TRY(lob_residual(c, phi, B, k, alpha, res));
     double rmax = 0.0;
-    for (int i = 0; i < k; i++) {
-      res[i] = std::sqrt(std::max(0.0, G[(size_t)i * k + i]));
-      rmax = std::max(rmax, res[i]);
-    }
+    for (int i = 0; i < k; i++) rmax = std::max(rmax, res[i]);
     if (it >= maxiter || (tol > 0 && rmax <= tol)) break;
     if (spm_cancelled(c)) return spm_fail(SPM_ERR_CANCELLED, "cancelled");
-    // W = P0(precond(W)), W perp V, W Gram-Schmidt with dropping (LOBPCG.cpp:287-308)
-    SPM_TRY(precond_many(c, W.data(), k));
-    SPM_TRY(project_out(c, Vc.data(), k, W.data(), k));
-    std::vector<int> keepW(k, 1), keepP(k, 0);
-    SPM_TRY(orth_with_drop(c, W.data(), k, 1e-8, keepW));
-    SPM_TRY(hv_many(c, phi, W.data(), Y.data(), k));
-    // P perp [V, W], Gram-Schmidt with dropping, Up = H P (LOBPCG.cpp:311-330)
-    if (have_p) {
-      std::vector<void *> VW(2 * k);
-      for (int i = 0; i < k; i++) {
-        VW[i] = Vc[i];
-        VW[k + i] = W[i];
-      }
-      SPM_TRY(project_out(c, VW.data(), 2 * k, P.data(), k));
-      keepP.assign(k, 1);
-      SPM_TRY(orth_with_drop(c, P.data(), k, 1e-8, keepP));
-      SPM_TRY(hv_many(c, phi, P.data(), Up.data(), k));
-    }
-    // Rayleigh-Ritz on S = [V; W; P] (kept vectors), LOBPCG.cpp:332-403
-    std::vector<void *> S, HS;
-    for (int i = 0; i < k; i++) {
-      S.push_back(Vc[i]);
-      HS.push_back(U[i]);
-    }
-    for (int i = 0; i < k; i++)
-      if (keepW[i]) {
-        S.push_back(W[i]);
-        HS.push_back(Y[i]);
-      }
-    for (int i = 0; i < k; i++)
-      if (keepP[i]) {
-        S.push_back(P[i]);
-        HS.push_back(Up[i]);
-      }
-    const int m = (int)S.size();
-    SPM_TRY(gram(c, S.data(), m, HS.data(), m, G));
-    std::vector<double> Gs((size_t)m * m), vals, vecs;
-    for (int i = 0; i < m; i++)
-      for (int j = 0; j < m; j++) Gs[(size_t)i * m + j] = (G[(size_t)j * m + i] + G[(size_t)i * m + j]) * 0.5;
-    sym_eig(Gs, m, vals, vecs);
-    // V_new = eta_k^T S; P <- V_old (LOBPCG.cpp:391-419)
-    std::vector<double> C((size_t)m * k);
-    for (int p = 0; p < m; p++)
-      for (int q = 0; q < k; q++) C[(size_t)p * k + q] = vecs[(size_t)p * m + q];
-    SPM_TRY(combine(c, S.data(), m, Vn.data(), k, C, nullptr, false));
-    std::swap(P, Vc);   // P holds the old V
-    std::swap(Vc, Vn);  // V holds the new block
-    have_p = true;
-    // mean removal and Gram-Schmidt of the new block (LOBPCG.cpp:428-449)
-    std::vector<double> mu;
-    SPM_TRY(means(c, Vc.data(), k, mu));
-    std::vector<double> I((size_t)k * k, 0.0), d(k);
-    for (int i = 0; i < k; i++) {
-      I[(size_t)i * k + i] = 1.0;
-      d[i] = -mu[i];
-    }
-    SPM_TRY(combine(c, Vc.data(), k, Vc.data(), k, I, &d, false));
-    SPM_TRY(orthonormalize(c, Vc.data(), k));
+    SPM_TRY(lob_update(c, phi, B, k, have_p));
   }
   // the caller's buffer receives the final block
-  for (int i = 0; i < k; i++) SPM_TRY(copy_fields(c, fld(c, V, i), Vc[i], 1));
+  for (int i = 0; i < k; i++) SPM_TRY(copy_fields(c, fld(c, V, i), B.Vc[i], 1));
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "lobpcg");
   if (evals) std::copy(alpha.begin(), alpha.end(), evals);
@@ -625,5 +653,79 @@ extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int 
   if (left > 0) SPM_TRY(spm_spring_pairing(c, phi0, phi1, left, tol, res_hist ? res_hist + n32 : nullptr, &n64));
   if (iters_fp32) *iters_fp32 = n32;
   if (iters_fp64) *iters_fp64 = n64;
+  return SPM_OK;
+}
+
+// ------------------------------------------------------------------ HiSD
+// hiosd_lobpcg_sieh (HISD.cpp:86-485): k-index saddle dynamics. Per iteration
+// a Barzilai-Borwein step size beta from the last position change Dx and the
+// change of the reflected force g = f - 2 PV(f) (clamped to [betau dt,
+// betat dt]); the semi-implicit position step along g (spectrum made real,
+// k = 0 removed, as the reference does); one LOBPCG iteration of the k
+// unstable directions V at the new position (the previous V kept as the P
+// block); then f = ngrad(x) and res = nrmp(f), stopping when res < epsf.
+extern "C" int spm_hisd(spm_ctx *c, void *x, void *V, int k, double dt, double betat, double betau, double epsf,
+                        int maxiter, double *res_hist, int *iters) {
+  if (!c || !x || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
+  if (iters) *iters = 0;
+  SPM_TRY(ensure_base(c));
+  SPM_TRY(spm_ensure_scratch(c, 1));  // the transform chains below (ngrad, the position step) use it
+  Solver *s = solver(c);
+  if (!s->hisd) {
+    cudaError_t e = cudaMalloc(&s->hisd, c->field_bytes * 6);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "HiSD work fields");
+  }
+  void *f = fld(c, s->hisd, 0), *tm = fld(c, s->hisd, 1), *g = fld(c, s->hisd, 2), *gp = fld(c, s->hisd, 3),
+       *Dx = fld(c, s->hisd, 4), *Dg = fld(c, s->hisd, 5);
+  const OpsTable *t = spm_table_of(c);
+  LobBlocks B;
+  SPM_TRY(lob_blocks(c, V, k, B));
+  std::vector<double> alpha(k, 0.0), res(k, 0.0), G;
+  auto pv = [&](double scale) -> int {  // tm = scale * sum_i <f, v_i> v_i (PV_Cplx, BasicOperators.cpp:360-371)
+    SPM_TRY(gram(c, B.Vc.data(), k, &f, 1, G));
+    std::vector<double> C(k);
+    for (int i = 0; i < k; i++) C[i] = scale * G[i];
+    return combine(c, B.Vc.data(), k, &tm, 1, C, nullptr, false);
+  };
+  auto lin2 = [&](void *out, double a, void *p, double b, void *q) -> int {  // FuncsLinear2Cplx
+    void *X[2] = {p, q};
+    std::vector<double> C = {a, b};
+    return combine(c, X, 2, &out, 1, C, nullptr, false);
+  };
+  SPM_TRY(orthonormalize(c, B.Vc.data(), k));  // HISD.cpp:151-157
+  SPM_TRY(t->ngrad(c, x, f));
+  SPM_TRY(zero_fields(c, gp, 1));
+  SPM_TRY(pv(1.0));
+  SPM_TRY(lin2(Dx, 1.0, f, -2.0, tm));
+  {  // FuncRealAddAConst(Dx, dt) (HISD.cpp:180)
+    std::vector<double> I = {1.0}, d = {dt};
+    SPM_TRY(combine(c, &Dx, 1, &Dx, 1, I, &d, false));
+  }
+  bool have_p = false;
+  int it = 0;
+  for (; it < maxiter;) {
+    SPM_TRY(pv(2.0));
+    SPM_TRY(lin2(g, 1.0, f, -1.0, tm));
+    SPM_TRY(lin2(Dg, 1.0, g, -1.0, gp));
+    SPM_TRY(copy_fields(c, gp, g, 1));
+    void *DD[2] = {Dx, Dg};
+    SPM_TRY(gram(c, DD, 2, &Dg, 1, G));  // <Dx, Dg>, <Dg, Dg>
+    double bta = std::fabs(G[0] / G[1]);
+    bta = std::min(bta, betat * dt);
+    bta = std::max(bta, betau * dt);
+    SPM_TRY(t->hisd_step(c, x, tm, Dx, bta));
+    SPM_TRY(lob_residual(c, x, B, k, alpha, res));
+    SPM_TRY(lob_update(c, x, B, k, have_p));
+    double gn = 0;
+    SPM_TRY(spm_ngrad(c, x, f, &gn));
+    if (res_hist) res_hist[it] = gn;
+    it++;
+    if (spm_cancelled(c)) return spm_fail(SPM_ERR_CANCELLED, "cancelled");
+    if (gn < epsf) break;
+  }
+  for (int i = 0; i < k; i++) SPM_TRY(copy_fields(c, fld(c, V, i), B.Vc[i], 1));
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "hisd");
+  if (iters) *iters = it;
   return SPM_OK;
 }

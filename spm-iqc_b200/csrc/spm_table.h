@@ -20,6 +20,7 @@ struct OpsTable {
   int (*tangent)(spm_ctx *, const void *phi0, const void *phi1, void *v_out, void *vhat, void *gv);
   int (*force)(spm_ctx *, void *const *x, int n, const void *v, const void *vhat, const void *gv, double factor);
   int (*gnorm)(spm_ctx *, const void *const *x, int n);
+  int (*hisd_step)(spm_ctx *, void *x, const void *t, void *dx, double beta);
 };
 
 // prec: 0 = FP64, 1 = FP32

@@ -280,6 +280,19 @@ class SpmContext:
         return np.array(ev[:]), np.array(rs[:]), it.value
 
     # ---- SPM.cpp
+    def hiosd_lobpcg_sieh(self, x, V, dt: float = 0.8, betat: float = 8.0, betau: float = 0.02,
+                          epsf: float = 1e-7, maxiter: int = 10000):
+        """HiSD (HISD.cpp:86-485) on (x, V) in place; returns the ||grad F|| history."""
+        f = lib().spm_hisd
+        f.argtypes = [_vp, _vp, _vp, ctypes.c_int] + [ctypes.c_double] * 4 + \
+            [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+        hist = (ctypes.c_double * max(1, maxiter))()
+        it = ctypes.c_int()
+        k = V.shape[0] if V.dim() == 4 else 1
+        check(f(self.h, _ptr(x), _ptr(V), k, float(dt), float(betat), float(betau), float(epsf), int(maxiter),
+                hist, ctypes.byref(it)))
+        return np.array(hist[:it.value])
+
     def get_Tv(self, phi0, phi1, v=None):
         v = self.field() if v is None else v
         check(lib().spm_get_tv(self.h, _ptr(phi0), _ptr(phi1), _ptr(v)))

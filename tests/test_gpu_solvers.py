@@ -119,3 +119,25 @@ def test_spring_pairing_stops_at_tolerance(spm, cuda):
     p0, p1 = t(cuda, phi), t(cuda, phi + 0.001 * vr)
     hist = ctx.Spring_Pairing(p0, p1, 50, 1e3)  # the first residual is below the tolerance
     assert len(hist) == 1
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_hisd_matches_oracle(spm, cuda, k):
+    """HiSD (hiosd_lobpcg_sieh, HISD.cpp:86-485) on the device against the FP64
+    oracle: positions, unstable directions (up to sign) and the ||grad F||
+    history after 8 iterations."""
+    N = 32
+    m = npo.Model(N, L=10.0, Tau=-0.05)
+    x0 = npo.uniform_field(N, 3) + 0.05 * np.cos(2 * np.pi * np.arange(N) / N)[:, None, None]
+    V0 = m.lobpcg_init(k, 5)
+    xo, Vo, ho = m.hisd(x0, V0, maxiter=8, epsf=1e-30)
+    ctx = spm.SpmContext(N, L=10.0, Tau=-0.05)
+    x = cuda.from_numpy(x0.copy()).cuda()
+    V = cuda.from_numpy(V0.copy()).cuda()
+    h = ctx.hiosd_lobpcg_sieh(x, V, maxiter=8, epsf=1e-30)
+    assert len(h) == 8
+    assert np.max(np.abs(h - ho) / ho) < 1e-9
+    assert rel(x.cpu().numpy(), xo) < 1e-10
+    Vg = V.cpu().numpy()
+    for i in range(k):
+        assert min(rel(Vg[i], Vo[i]), rel(-Vg[i], Vo[i])) < 1e-8, i

@@ -142,3 +142,23 @@ def test_splitmix_uniform_matches_shim_stream():
     import inputs
     idx = np.arange(10, dtype=np.uint64)
     assert np.array_equal(npo.uniform_pm1(5, idx), -1.0 + 2.0 * inputs.unit(5, idx))
+
+
+def test_hisd_restatement_matches_reference():
+    """hiosd_lobpcg_sieh (HISD.cpp:86-485): the NumPy restatement against the
+    reference compiled in place, 1 and 8 iterations, k = 1 and 2."""
+    if not refbind.available():
+        pytest.skip("compiled reference not built")
+    N = 16
+    m = npo.Model(N, L=10.0, Tau=-0.05)
+    x = npo.uniform_field(N, 3) + 0.05 * np.cos(2 * np.pi * np.arange(N) / N)[:, None, None]
+    r = refbind.Ref(N, L=10.0, Tau=-0.05)
+    for k, its in ((1, 1), (1, 8), (2, 8)):
+        V = m.lobpcg_init(k, 5)
+        xr, Vr = r.hisd(x, V, maxiter=its, epsf=1e-30)
+        xo, Vo, _ = m.hisd(x, V, maxiter=its, epsf=1e-30)
+        assert np.max(np.abs(xr - xo)) <= 1e-12 * np.max(np.abs(xo))
+        for i in range(k):  # eigenvectors up to sign
+            d = min(np.max(np.abs(Vr[i] - Vo[i])), np.max(np.abs(Vr[i] + Vo[i])))
+            assert d <= 1e-9, (k, its, i, d)
+    r.close()
