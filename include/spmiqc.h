@@ -234,6 +234,11 @@ int spm_spring_pairing_mixed(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, 
  * NULL, >= maxiter entries) receives ||grad F|| per iteration. */
 int spm_hisd(spm_ctx *ctx, void *x, void *V, int k, double dt, double betat, double betau, double epsf,
              int maxiter, double *res_hist, int *iters);
+/* hiosd_lobpcg_sieh_V0 (GOSD.cpp:123-531): spm_hisd with the directions V
+ * also kept orthogonal to k0 fixed orthonormal fields V0 (1 <= k0 <= 24), as
+ * critical_point (GOSD.cpp:13-56) does with the zero modes of a structure. */
+int spm_gosd(spm_ctx *ctx, void *x, void *V, int k, const void *V0, int k0, double dt, double betat, double betau,
+             double epsf, int maxiter, double *res_hist, int *iters);
 
 /* ------------------------------------------------------------ BLAS-1 */
 

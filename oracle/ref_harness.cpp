@@ -23,6 +23,7 @@
 #include "BasicOperators.h"
 #include "Data.h"
 #include "File_Op.h"
+#include "GOSD.h"
 #include "HISD.h"
 #include "Initialization.h"
 #include "LOBPCG.h"
@@ -356,6 +357,42 @@ void ref_hisd(double *xr, int k, double *V, double dt, double betat, double beta
   }
   to_real(x, xr);
   for (int i = 0; i < k; i++) to_real(g_opt->V[i], V + (size_t)i * CplxDofs_local);
+  free(x);
+}
+
+// GOSD.cpp:123-531 (hiosd_lobpcg_sieh_V0) on (x, V) with k0 fixed fields V0.
+void ref_gosd(double *xr, int k, double *V, int k0, const double *V0r, double dt, double betat, double betau,
+              double epsf, int maxiter) {
+  if (!g_opt || g_opt->k != k) {
+    free_option();
+    spm_shim_eigen_seed(0);
+    g_opt = (Option *)malloc(sizeof(Option));
+    Mute m;
+    hiosd_lobpcg_initialization(g_opt, k);
+  }
+  for (int i = 0; i < k; i++) to_cplx(V + (size_t)i * CplxDofs_local, g_opt->V[i]);
+  g_opt->dt = dt;
+  g_opt->betat = betat;
+  g_opt->betau = betau;
+  g_opt->epsf = epsf;
+  g_opt->maxiter = maxiter;
+  g_opt->outputp = 100;
+  g_opt->outputd = 1000;
+  fftw_complex **V0 = (fftw_complex **)malloc(sizeof(fftw_complex *) * k0);
+  for (int i = 0; i < k0; i++) {
+    V0[i] = alloc_c();
+    to_cplx(V0r + (size_t)i * CplxDofs_local, V0[i]);
+  }
+  fftw_complex *x = alloc_c();
+  to_cplx(xr, x);
+  {
+    Mute m;
+    hiosd_lobpcg_sieh_V0(x, g_opt, V0, k0);
+  }
+  to_real(x, xr);
+  for (int i = 0; i < k; i++) to_real(g_opt->V[i], V + (size_t)i * CplxDofs_local);
+  for (int i = 0; i < k0; i++) free(V0[i]);
+  free(V0);
   free(x);
 }
 

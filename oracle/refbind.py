@@ -67,6 +67,7 @@ def lib(path: str = LIB):
         L.ref_load_option_v.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
         L.ref_initial_value.argtypes = [ctypes.c_int, ctypes.c_char_p, _dp]
         L.ref_hisd.argtypes = [_dp, ctypes.c_int, _dp] + [ctypes.c_double] * 4 + [ctypes.c_int]
+        L.ref_gosd.argtypes = [_dp, ctypes.c_int, _dp, ctypes.c_int, _dp] + [ctypes.c_double] * 4 + [ctypes.c_int]
         _libs[path] = L
     return _libs[path]
 
@@ -176,6 +177,14 @@ class Ref:
         x = np.array(x, dtype=np.float64, order="C")
         V = np.array(V, dtype=np.float64, order="C")
         self.L.ref_hisd(_p(x), V.shape[0], _p(V), dt, betat, betau, epsf, int(maxiter))
+        return x, V
+
+    def gosd(self, x, V, V0, dt=0.8, betat=8.0, betau=1.3, epsf=1e-9, maxiter=40000):
+        """hiosd_lobpcg_sieh_V0 on copies of (x, V) with the fixed fields V0."""
+        x = np.array(x, dtype=np.float64, order="C")
+        V = np.array(V, dtype=np.float64, order="C")
+        V0 = np.ascontiguousarray(V0, dtype=np.float64)
+        self.L.ref_gosd(_p(x), V.shape[0], _p(V), V0.shape[0], _p(V0), dt, betat, betau, epsf, int(maxiter))
         return x, V
 
     # File_Op.cpp: the reference's field files

@@ -232,9 +232,10 @@ class Model:
                 V[i] *= 1.0 / self.nrmp(V[i])
         return V, ritz
 
-    def _lob_step(self, x, V, U, W, Y, Vp, Up):
+    def _lob_step(self, x, V, U, W, Y, Vp, Up, V0=None):
         """One iteration body of src/HISD.cpp:258-444 (the LOBPCG update of V
-        at position x, with the previous V as the P block); returns the new V."""
+        at position x, with the previous V as the P block); returns the new V.
+        With V0 (src/GOSD.cpp:298-326) W, Vp and V are also kept orthogonal to V0."""
         k = V.shape[0]
         shape = V.shape
         emp = np.ones(3 * k, dtype=bool)
@@ -244,6 +245,8 @@ class Model:
             W[i] = 1 * U[i] + (-a) * V[i]
             W[i] = self.precond(W[i])
             self.orth_v2V(W[i], V, k)
+            if V0 is not None:
+                self.orth_v2V(W[i], V0, V0.shape[0])
             self.orth_Vi(W, i)
             nw = self.nrmp(W[i])
             if nw > 1e-8:
@@ -256,6 +259,8 @@ class Model:
         for i in range(k):
             self.orth_v2V(Vp[i], V, k)
             self.orth_v2V(Vp[i], W, k)
+            if V0 is not None:
+                self.orth_v2V(Vp[i], V0, V0.shape[0])
             self.orth_Vi(Vp, i)
             nv = self.nrmp(Vp[i])
             if nv > 1e-8:
@@ -277,11 +282,14 @@ class Model:
             V[i] -= np.sum(V[i]) / self.n3
         for i in range(k):
             self.orth_v2V(V[i], V, i)
+            if V0 is not None:
+                self.orth_v2V(V[i], V0, V0.shape[0])
             V[i] *= 1.0 / self.nrmp(V[i])
         return V
 
-    # src/HISD.cpp:86-485 (hiosd_lobpcg_sieh)
-    def hisd(self, x, V, dt=0.8, betat=8.0, betau=0.02, epsf=1e-7, maxiter=10000):
+    # src/HISD.cpp:86-485 (hiosd_lobpcg_sieh); with V0, src/GOSD.cpp:123-531
+    # (hiosd_lobpcg_sieh_V0)
+    def hisd(self, x, V, dt=0.8, betat=8.0, betau=0.02, epsf=1e-7, maxiter=10000, V0=None):
         """Returns (x, V, residual history)."""
         k = V.shape[0]
         x = x.copy()
@@ -311,7 +319,7 @@ class Model:
             rho[0, 0, 0] = 0.0
             x = self.my_ifft(rho).real
             Dx = x - xp
-            V = self._lob_step(x, V, U, W, Y, Vp, Up)
+            V = self._lob_step(x, V, U, W, Y, Vp, Up, V0)
             f = self.ngrad(x)
             res = self.nrmp(f)
             hist.append(res)

@@ -405,10 +405,14 @@ static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::v
 // Gram-Schmidt and the 1e-8 dropping, Y = H W; P perp [V, W], dropping,
 // Up = H P; Rayleigh-Ritz on [V; W; P]; P <- V; V <- the k lowest Ritz
 // vectors, mean removed and Gram-Schmidt orthonormalised.
-static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &have_p) {
+// With V0 (k0 fixed orthonormal fields, GOSD.cpp) W, P and the new V are also
+// kept orthogonal to V0.
+static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &have_p, void *const *V0 = nullptr,
+                      int k0 = 0) {
   std::vector<double> G;
   SPM_TRY(precond_many(c, B.W.data(), k));
   SPM_TRY(project_out(c, B.Vc.data(), k, B.W.data(), k));
+  if (k0 > 0) SPM_TRY(project_out(c, V0, k0, B.W.data(), k));
   std::vector<int> keepW(k, 1), keepP(k, 0);
   SPM_TRY(orth_with_drop(c, B.W.data(), k, 1e-8, keepW));
   SPM_TRY(hv_many(c, phi, B.W.data(), B.Y.data(), k));
@@ -419,6 +423,7 @@ static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &ha
       VW[k + i] = B.W[i];
     }
     SPM_TRY(project_out(c, VW.data(), 2 * k, B.P.data(), k));
+    if (k0 > 0) SPM_TRY(project_out(c, V0, k0, B.P.data(), k));
     keepP.assign(k, 1);
     SPM_TRY(orth_with_drop(c, B.P.data(), k, 1e-8, keepP));
     SPM_TRY(hv_many(c, phi, B.P.data(), B.Up.data(), k));
@@ -459,6 +464,7 @@ static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &ha
     d[i] = -mu[i];
   }
   SPM_TRY(combine(c, B.Vc.data(), k, B.Vc.data(), k, I, &d, false));
+  if (k0 > 0) SPM_TRY(project_out(c, V0, k0, B.Vc.data(), k));
   return orthonormalize(c, B.Vc.data(), k);
 }
 
@@ -664,9 +670,12 @@ extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int 
 // k = 0 removed, as the reference does); one LOBPCG iteration of the k
 // unstable directions V at the new position (the previous V kept as the P
 // block); then f = ngrad(x) and res = nrmp(f), stopping when res < epsf.
-extern "C" int spm_hisd(spm_ctx *c, void *x, void *V, int k, double dt, double betat, double betau, double epsf,
-                        int maxiter, double *res_hist, int *iters) {
-  if (!c || !x || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0) return spm_fail(SPM_ERR_ARG, "bad argument");
+static int hisd_run(spm_ctx *c, void *x, void *V, int k, const void *V0p, int k0, double dt, double betat,
+                    double betau, double epsf, int maxiter, double *res_hist, int *iters) {
+  if (!c || !x || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0 || k0 < 0 || k0 > kBlkMax || (k0 && !V0p))
+    return spm_fail(SPM_ERR_ARG, "bad argument");
+  std::vector<void *> V0(k0);
+  for (int i = 0; i < k0; i++) V0[i] = fld(c, const_cast<void *>(V0p), i);
   if (iters) *iters = 0;
   SPM_TRY(ensure_base(c));
   SPM_TRY(spm_ensure_scratch(c, 1));  // the transform chains below (ngrad, the position step) use it
@@ -715,7 +724,7 @@ extern "C" int spm_hisd(spm_ctx *c, void *x, void *V, int k, double dt, double b
     bta = std::max(bta, betau * dt);
     SPM_TRY(t->hisd_step(c, x, tm, Dx, bta));
     SPM_TRY(lob_residual(c, x, B, k, alpha, res));
-    SPM_TRY(lob_update(c, x, B, k, have_p));
+    SPM_TRY(lob_update(c, x, B, k, have_p, V0.data(), k0));
     double gn = 0;
     SPM_TRY(spm_ngrad(c, x, f, &gn));
     if (res_hist) res_hist[it] = gn;
@@ -728,4 +737,18 @@ extern "C" int spm_hisd(spm_ctx *c, void *x, void *V, int k, double dt, double b
   if (e != cudaSuccess) return spm_fail_cuda(e, "hisd");
   if (iters) *iters = it;
   return SPM_OK;
+}
+
+extern "C" int spm_hisd(spm_ctx *c, void *x, void *V, int k, double dt, double betat, double betau, double epsf,
+                        int maxiter, double *res_hist, int *iters) {
+  return hisd_run(c, x, V, k, nullptr, 0, dt, betat, betau, epsf, maxiter, res_hist, iters);
+}
+
+// hiosd_lobpcg_sieh_V0 (GOSD.cpp:123-531): HiSD with the unstable directions
+// also kept orthogonal to a fixed orthonormal subspace V0 (k0 fields, e.g. the
+// zero modes of a structure, critical_point, GOSD.cpp:13-56).
+extern "C" int spm_gosd(spm_ctx *c, void *x, void *V, int k, const void *V0, int k0, double dt, double betat,
+                        double betau, double epsf, int maxiter, double *res_hist, int *iters) {
+  if (k0 < 1 || !V0) return spm_fail(SPM_ERR_ARG, "GOSD needs k0 >= 1 fixed fields");
+  return hisd_run(c, x, V, k, V0, k0, dt, betat, betau, epsf, maxiter, res_hist, iters);
 }

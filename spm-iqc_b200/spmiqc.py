@@ -293,6 +293,20 @@ class SpmContext:
                 hist, ctypes.byref(it)))
         return np.array(hist[:it.value])
 
+    def hiosd_lobpcg_sieh_V0(self, x, V, V0, dt: float = 0.8, betat: float = 8.0, betau: float = 1.3,
+                             epsf: float = 1e-9, maxiter: int = 40000):
+        """GOSD (GOSD.cpp:123-531): HiSD with V kept orthogonal to the fixed fields V0; returns the history."""
+        f = lib().spm_gosd
+        f.argtypes = [_vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int] + [ctypes.c_double] * 4 + \
+            [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+        hist = (ctypes.c_double * max(1, maxiter))()
+        it = ctypes.c_int()
+        k = V.shape[0] if V.dim() == 4 else 1
+        k0 = V0.shape[0] if V0.dim() == 4 else 1
+        check(f(self.h, _ptr(x), _ptr(V), k, _ptr(V0), k0, float(dt), float(betat), float(betau), float(epsf),
+                int(maxiter), hist, ctypes.byref(it)))
+        return np.array(hist[:it.value])
+
     def get_Tv(self, phi0, phi1, v=None):
         v = self.field() if v is None else v
         check(lib().spm_get_tv(self.h, _ptr(phi0), _ptr(phi1), _ptr(v)))

@@ -141,3 +141,24 @@ def test_hisd_matches_oracle(spm, cuda, k):
     Vg = V.cpu().numpy()
     for i in range(k):
         assert min(rel(Vg[i], Vo[i]), rel(-Vg[i], Vo[i])) < 1e-8, i
+
+
+def test_gosd_matches_oracle(spm, cuda):
+    """GOSD (hiosd_lobpcg_sieh_V0, GOSD.cpp:123-531) on the device against the
+    FP64 oracle, with two fixed directions V0; V stays orthogonal to V0."""
+    N = 32
+    m = npo.Model(N, L=10.0, Tau=-0.05)
+    x0 = npo.uniform_field(N, 3) + 0.05 * np.cos(2 * np.pi * np.arange(N) / N)[:, None, None]
+    V00, _ = m.lobpcg_inip(x0, m.lobpcg_init(2, 9), 6)
+    Vs = m.lobpcg_init(1, 5)
+    xo, Vo, ho = m.hisd(x0, Vs, betau=0.02, maxiter=6, epsf=1e-30, V0=V00)
+    ctx = spm.SpmContext(N, L=10.0, Tau=-0.05)
+    x = cuda.from_numpy(x0.copy()).cuda()
+    V = cuda.from_numpy(Vs.copy()).cuda()
+    V0 = cuda.from_numpy(np.ascontiguousarray(V00)).cuda()
+    h = ctx.hiosd_lobpcg_sieh_V0(x, V, V0, betau=0.02, maxiter=6, epsf=1e-30)
+    assert len(h) == 6 and np.max(np.abs(h - ho) / ho) < 1e-9
+    assert rel(x.cpu().numpy(), xo) < 1e-10
+    Vg = V.cpu().numpy()
+    assert min(rel(Vg[0], Vo[0]), rel(-Vg[0], Vo[0])) < 1e-8
+    assert max(abs(m.inpfp(Vg[0], V00[i])) for i in range(2)) < 1e-12

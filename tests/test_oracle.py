@@ -162,3 +162,23 @@ def test_hisd_restatement_matches_reference():
             d = min(np.max(np.abs(Vr[i] - Vo[i])), np.max(np.abs(Vr[i] + Vo[i])))
             assert d <= 1e-9, (k, its, i, d)
     r.close()
+
+
+def test_gosd_restatement_matches_reference():
+    """hiosd_lobpcg_sieh_V0 (GOSD.cpp:123-531): HiSD with the directions kept
+    orthogonal to a fixed subspace V0 (here the two lowest Hessian modes at
+    the start), NumPy restatement against the compiled reference."""
+    if not refbind.available():
+        pytest.skip("compiled reference not built")
+    N = 16
+    m = npo.Model(N, L=10.0, Tau=-0.05)
+    x = npo.uniform_field(N, 3) + 0.05 * np.cos(2 * np.pi * np.arange(N) / N)[:, None, None]
+    V0, _ = m.lobpcg_inip(x, m.lobpcg_init(2, 9), 6)
+    V = m.lobpcg_init(1, 5)
+    r = refbind.Ref(N, L=10.0, Tau=-0.05)
+    xr, Vr = r.gosd(x, V, V0, betau=0.02, maxiter=6, epsf=1e-30)
+    xo, Vo, _ = m.hisd(x, V, betau=0.02, maxiter=6, epsf=1e-30, V0=V0)
+    r.close()
+    assert np.max(np.abs(xr - xo)) <= 1e-12 * np.max(np.abs(xo))
+    assert min(np.max(np.abs(Vr[0] - Vo[0])), np.max(np.abs(Vr[0] + Vo[0]))) <= 1e-9
+    assert abs(m.inpfp(Vo[0], V0[0])) < 1e-12 and abs(m.inpfp(Vo[0], V0[1])) < 1e-12
