@@ -144,9 +144,11 @@ int spm_grad_flow_mixed(spm_ctx *ctx, void *phi, void *uhat, int max_steps, doub
  * captured CUDA graph advances every instance by steps_per_launch gated steps
  * on parallel stream branches and is relaunched until all instances reached
  * ||grad F|| <= tol_grad (or max_steps). With switch_tol > tol_grad the
- * instances (FP64 contexts) first run with FP32 transforms to switch_tol,
- * then in FP64. steps_done (host, n entries, may be NULL) receives the steps
- * executed per instance. The contexts' streams are synchronised first. */
+ * instances (FP64 contexts) first run with FP32 transforms to switch_tol (or
+ * until 512 FP32 steps bring no new minimum of ||grad F||), then in FP64 with
+ * the steps each has left. steps_done (host, n entries, may be NULL) receives
+ * the steps executed per instance. The contexts' streams are synchronised
+ * first. */
 int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n, int max_steps, double tol_grad,
                         double switch_tol, int steps_per_launch, int *steps_done);
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "../../include/spmiqc.h"
@@ -36,8 +37,12 @@ struct Streams {
 };
 
 // Runs the flows of n contexts to tol (or max_steps each); steps[i] += done.
+// With stall > 0 an instance is also stopped (between graph launches) once
+// `stall` of its steps have brought no new minimum of ||grad F|| (the FP32
+// rounding floor of a mixed run).
+// caps (may be null) gives each instance its own step budget (<= max_steps).
 int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int max_steps, double tol, int K,
-              int *steps) {
+              int *steps, int stall = 0, const int *caps = nullptr) {
   Streams st;
   st.s.resize(n + 1);
   st.ev.resize(n + 1);
@@ -55,7 +60,7 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     SPM_TRY(spm_ensure_stats(ctx[i], max_steps + K));
     SPM_TRY(spm_flow_init(ctx[i], s0));
     ctx[i]->m.tol_grad = tol;
-    ctx[i]->m.max_steps = max_steps;
+    ctx[i]->m.max_steps = caps ? caps[i] : max_steps;
   }
   // one step of every instance outside the capture sets up kernel attributes
   // and tensor maps; it counts as the first step of the flow
@@ -89,6 +94,9 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     return spm_fail_cuda(e, "graph instantiate");
   }
   std::vector<int> host(8 * (size_t)n);
+  std::vector<double> best(n, INFINITY), rec;
+  std::vector<int> seen(n, 1), last_better(n, 0);  // the step outside the graph is record 0
+  static const int kZero = 0;
   const int launches = (max_steps + K - 1) / K;
   for (int l = 0; l < launches && rc == SPM_OK; l++) {
     e = cudaGraphLaunch(exec, s0);
@@ -106,9 +114,36 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     bool all = true;
     for (int i = 0; i < n; i++) {
       if (host[8 * (size_t)i + FW_ERR]) rc = spm_fail(SPM_ERR_CUDA, "a bounded wait timed out in a batched flow");
+      if (stall > 0 && host[8 * (size_t)i + FW_GO] != 0) {
+        const int it = host[8 * (size_t)i + FW_ITER];
+        if (it > seen[i]) {
+          rec.resize(4 * (size_t)(it - seen[i]));
+          e = cudaMemcpy(rec.data(), ctx[i]->stats + 4 * (size_t)seen[i], sizeof(double) * rec.size(),
+                         cudaMemcpyDeviceToHost);
+          if (e != cudaSuccess) {
+            rc = spm_fail_cuda(e, "batch records");
+            break;
+          }
+          for (int s = 0; s < it - seen[i]; s++)
+            if (rec[4 * (size_t)s + 2] < best[i]) {
+              best[i] = rec[4 * (size_t)s + 2];
+              last_better[i] = seen[i] + s;
+            }
+          seen[i] = it;
+          if (it - last_better[i] >= stall) {  // the instance stops before the next launch
+            e = cudaMemcpyAsync(ctx[i]->flow + FW_GO, &kZero, sizeof(int), cudaMemcpyHostToDevice, s0);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
+            if (e != cudaSuccess) {
+              rc = spm_fail_cuda(e, "batch stop");
+              break;
+            }
+            host[8 * (size_t)i + FW_GO] = 0;
+          }
+        }
+      }
       all = all && host[8 * (size_t)i + FW_GO] == 0;
     }
-    if (all) break;
+    if (all || rc != SPM_OK) break;
   }
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
@@ -147,7 +182,7 @@ extern "C" int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n
       c->launches += 2;
     }
     SPM_TRY(run_phase(tw.data(), p32.data(), u32.data(), n, max_steps, switch_tol, steps_per_launch,
-                      steps.data()));
+                      steps.data(), 512));
     for (int i = 0; i < n; i++) {
       spm_ctx *c = ctx[i];
       const size_t m = (size_t)c->N * c->N * c->N;
@@ -156,10 +191,25 @@ extern "C" int spm_batch_grad_flow(spm_ctx **ctx, void **phi, void **uhat, int n
       SPM_TRY(spm_fft(c, phi[i], uhat[i]));
     }
   }
-  int left = max_steps;
-  for (int i = 0; i < n; i++) left = std::min(left, max_steps - steps[i]);
-  if (left > 0)
-    SPM_TRY(run_phase(ctx, phi, uhat, n, left, tol_grad, steps_per_launch, steps.data()));
+  // FP64 phase: each instance with steps left continues with its own budget
+  std::vector<spm_ctx *> c64;
+  std::vector<void *> p64, u64;
+  std::vector<int> caps, idx, s64;
+  for (int i = 0; i < n; i++)
+    if (max_steps - steps[i] > 0) {
+      c64.push_back(ctx[i]);
+      p64.push_back(phi[i]);
+      u64.push_back(uhat[i]);
+      caps.push_back(max_steps - steps[i]);
+      idx.push_back(i);
+    }
+  if (!c64.empty()) {
+    const int most = *std::max_element(caps.begin(), caps.end());
+    s64.assign(c64.size(), 0);
+    SPM_TRY(run_phase(c64.data(), p64.data(), u64.data(), (int)c64.size(), most, tol_grad, steps_per_launch,
+                      s64.data(), 0, caps.data()));
+    for (size_t j = 0; j < idx.size(); j++) steps[idx[j]] += s64[j];
+  }
   for (int i = 0; i < n; i++) {
     cudaError_t e = cudaStreamSynchronize(ctx[i]->stream);
     if (e != cudaSuccess) return spm_fail_cuda(e, "batch");

@@ -486,3 +486,17 @@ def load_checkpoint(path: str):
     out = np.empty((info.nfields, info.N, info.N, info.N))
     check(f(path.encode(), ctypes.byref(info), out.ctypes.data, out.size))
     return info, out
+
+
+def batch_grad_flow(ctxs, phis, uhats, max_steps: int, tol_grad: float, switch_tol: float = 0.0,
+                    steps_per_launch: int = 16):
+    """spm_batch_grad_flow: all instances advanced by one captured graph per launch; returns the steps per instance."""
+    n = len(ctxs)
+    f = lib().spm_batch_grad_flow
+    arr = ctypes.c_void_p * n
+    f.argtypes = [arr, arr, arr, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_int)]
+    done = (ctypes.c_int * n)()
+    check(f(arr(*[c.h.value for c in ctxs]), arr(*[_ptr(p) for p in phis]), arr(*[_ptr(u) for u in uhats]), n,
+            int(max_steps), float(tol_grad), float(switch_tol), int(steps_per_launch), done))
+    return list(done)

@@ -52,6 +52,19 @@ def serving_stream(seed: int, n_jobs: int, rate: float = 4.0, sizes=(64, 128, 19
     return out
 
 
+def batch_instances(seed: int, n: int = 24, sizes=(64, 96, 128, 160, 192, 256)):
+    """Batched-relaxation instances: N from `sizes` (each at least once when n
+    allows), L ~ U[18, 30], Tau ~ U[-0.02, 0], BCC / FCC / icosahedral shells,
+    amplitude ~ U[0.1, 0.2]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        N = sizes[i % len(sizes)] if i < len(sizes) else int(rng.choice(sizes))
+        out.append(JobSpec(0.0, "relax", N, float(rng.uniform(18, 30)), float(rng.uniform(-0.02, 0)),
+                           SHELLS[int(rng.integers(3))], float(rng.uniform(0.1, 0.2)), int(rng.integers(1 << 31))))
+    return out
+
+
 def shell_vectors(shell: str, L: float) -> np.ndarray:
     if shell == "bcc":
         return inputs.bcc_shell(L)

@@ -122,3 +122,26 @@ def test_spring_pairing_fp32_phase_tracks_fp64(cuda):
     assert i32 == 20 and i64 == 0 and len(hb) == len(ha) == 20
     assert np.max(np.abs(hb - ha) / ha) < 1e-4
     assert rel(b0.cpu().numpy(), a0.cpu().numpy()) < 1e-5 and rel(b1.cpu().numpy(), a1.cpu().numpy()) < 1e-5
+
+
+def test_batched_mixed_flows_reach_tolerance(cuda):
+    """spm_batch_grad_flow with an FP32 phase (switch 1e-7, stagnation stop)
+    and FP64 polish: every instance reaches ||grad F|| <= 1e-8 with the energy
+    of its all-FP64 single flow to 1e-10 of the initial energy."""
+    import spmiqc
+    specs = [(32, 26.0, -0.02, 1), (64, 20.0, -0.015, 2), (32, 18.0, -0.01, 3)]
+    ctxs, phis, uhs, ref = [], [], [], []
+    for N, L, tau, seed in specs:
+        c = spmiqc.SpmContext(N, L=L, Tau=tau)
+        p0 = npo.uniform_field(N, seed)
+        p = cuda.from_numpy(p0).cuda()
+        ctxs.append(c), phis.append(p), uhs.append(c.my_fft(p))
+        q = cuda.from_numpy(p0).cuda()
+        uq = c.my_fft(q)
+        E0 = c.get_Ene(q, uq)
+        c.get_min_u_F(q, uq, 60000, tol_grad=1e-8)
+        ref.append((E0, c.get_Ene(q, uq)))
+    spmiqc.batch_grad_flow(ctxs, phis, uhs, 60000, 1e-8, switch_tol=1e-7, steps_per_launch=32)
+    for c, p, u, (E0, E) in zip(ctxs, phis, uhs, ref):
+        assert c.ngrad_cam(p)[1] <= 1e-8 * 1.01
+        assert abs(c.get_Ene(p, u) - E) <= 1e-10 * abs(E0)
