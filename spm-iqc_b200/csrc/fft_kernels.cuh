@@ -169,12 +169,17 @@ template <int N, class T> struct Plane {
         v[j1] = rem[(y & 31) * M + col];
       });
       Dft<-1, M1, T2>::run(v);  // consumes every gathered value
-      // done reading the other CTAs' rows: they may overwrite them after the wait
+      // done reading the other CTAs' rows: they may overwrite them after the
+      // wait, which comes after the twiddles
       cluster_arrive_relaxed();
+      sfor<1, M1>([&](auto K1) {
+        constexpr int k1 = SPM_CI(K1);
+        v[k1] = cmul(v[k1], tw[j2 * k1]);
+      });
       cluster_wait();
       sfor<0, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
-        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmul(v[k1], tw[j2 * k1]);
+        buf[k1 * 256 + j2 * 16 + c] = v[k1];
       });
     }
     __syncthreads();
@@ -193,8 +198,12 @@ template <int N, class T> struct Plane {
     }
   }
 
+  // Position of (y, column c) in the inverse-y output: stage 2 of task
+  // (c, k1) writes its outputs y = k1 + M1*k2 back to the slots it read.
+  __device__ static int ycol(int y, int c) { return (y % M1) * 256 + (y / M1) * 16 + c; }
+
   // inverse y over this CTA's 16 columns; ld(ky, c) returns the input value.
-  // Leaves [y][16 columns] in buf and ends with a cluster barrier.
+  // Leaves y-line values at ycol(y, c) in buf and ends with a cluster barrier.
   template <class LD>
   __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld) {
     {
@@ -211,89 +220,76 @@ template <int N, class T> struct Plane {
       });
     }
     __syncthreads();
-    {
+    if (tid < 16 * M1) {
       T2 u[16];
       const int c = tid & 15, k1 = tid >> 4;
-      if (tid < 16 * M1) {
 #pragma unroll
-        for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
-        Dft<+1, 16, T2>::run(u);
-      }
-      __syncthreads();
-      if (tid < 16 * M1) {
+      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+      Dft<+1, 16, T2>::run(u);
 #pragma unroll
-        for (int k2 = 0; k2 < 16; k2++) buf[(k1 + M1 * k2) * 16 + c] = u[k2];
-      }
+      for (int k2 = 0; k2 < 16; k2++) buf[k1 * 256 + k2 * 16 + c] = u[k2];  // = ycol(k1 + M1*k2, c)
     }
     cluster.sync();
   }
 
-  // complex-to-real pre-processing: gather the pairs (q, M-q) of this CTA's
-  // rows from the column owners, then store the rows [r][M] (each warp its own
-  // rows, ready for zi1 of the same warp).
-  __device__ static void c2r_pre(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster) {
-    const int warp = tid >> 5, lane = tid & 31;
-    constexpr int NT = RPW * (M / 2);
-    constexpr int TPT = NT / 32;  // N/32 tasks per thread
-    static_assert(NT % 32 == 0, "task count");
-    T2 za[TPT], zb[TPT];
+  // Complex-to-real pre-processing fused with stage 1 of the inverse z
+  // transform. Thread (r, j2) (j2 = tid & 7, r = tid >> 3) transforms Z_q of
+  // row r for q = 8 j1 + j2. Z_q and Z_{M-q} come from the same two gathered
+  // values X_q, X_{M-q} (column owners, through distributed shared memory), and
+  // M - q = 8 (N1-1-j1) + (8-j2), so lanes j2 and (8-j2) & 7 of a row each
+  // build half of the pairs and swap the partner halves with shuffles (lane 0
+  // pairs q = 0 with M/2; lanes 0 and 4 are their own partners). The "done
+  // reading" arrive follows the last use of a gathered value and its wait
+  // comes only before the stores into the row, so the radix-N1 DFT runs in
+  // between. Ends with the z exchange of each row written (same warp).
+  __device__ static void c2r_zi1(T2 *buf, const T2 *tw, const T2 *ztw, int tid, int rank,
+                                 cg::cluster_group &cluster) {
+    constexpr int H = N1 / 2;
+    static_assert(N1 % 2 == 0, "pairs");
+    const int j2 = tid & 7, r = tid >> 3, lane = tid & 31;
+    const int y = rank * kRows + r;
+    T2 v[N1], w[H];
 #pragma unroll
-    for (int i = 0; i < TPT; i++) {
-      const int task = lane + 32 * i;
-      const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
-      const int y = rank * kRows + r;
+    for (int j = 0; j < H; j++) {
+      const int q = 8 * j + j2;
       if (q == 0) {
-        const T2 *r0 = cluster.map_shared_rank(buf, 0u);
-        const T2 *rh = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols));
-        const T2 P = r0[y * 16 + 0];
-        const T2 a = rh[y * 16 + (M / 2) % kCols];
+        const T2 P = cluster.map_shared_rank(buf, 0u)[ycol(y, 0)];
+        const T2 a = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols))[ycol(y, (M / 2) % kCols)];
         // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
-        za[i] = T2{P.x + P.y, P.x - P.y};
+        v[0] = T2{P.x + P.y, P.x - P.y};
         // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
         const T2 e = {a.x + a.x, (T)0};
         const T2 o = {(T)0, a.y + a.y};
-        zb[i] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
+        w[0] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
       } else {
-        const T2 *ra = cluster.map_shared_rank(buf, (unsigned)(q / kCols));
-        const T2 *rb = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols));
-        const T2 a = ra[y * 16 + q % kCols];
-        const T2 c = rb[y * 16 + (M - q) % kCols];
+        const T2 a = cluster.map_shared_rank(buf, (unsigned)(q / kCols))[ycol(y, q % kCols)];
+        const T2 c = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols))[ycol(y, (M - q) % kCols)];
         // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
         const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
         const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
-        za[i] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
-        zb[i] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
+        v[j] = cadd(e1, mul_di<+1>(cmulc(d1, tw[q])));
+        w[j] = cadd(e2, mul_di<+1>(cmulc(d2, tw[M - q])));
       }
     }
     // every gathered value is consumed: done reading the column owners
     cluster_arrive_relaxed();
-    cluster_wait();
+    const int src = (lane & ~7) | ((8 - j2) & 7);
 #pragma unroll
-    for (int i = 0; i < TPT; i++) {
-      const int task = lane + 32 * i;
-      const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
-      T2 *Z = buf + r * M;
-      if (q == 0) {
-        Z[0] = za[i];
-        Z[M / 2] = zb[i];
-      } else {
-        Z[q] = za[i];
-        Z[M - q] = zb[i];
-      }
+    for (int j = 0; j < H; j++) {
+      // the partner's w[j] is Z at j1 = N1-1-j of this lane; lane 0 (its own
+      // partner) holds Z_{M/2} in w[0], so it sends its pairs rotated by one
+      const T2 snd = (j2 == 0) ? w[(j + 1) % H] : w[j];
+      v[N1 - 1 - j] = T2{__shfl_sync(0xffffffffu, snd.x, src), __shfl_sync(0xffffffffu, snd.y, src)};
     }
-    __syncwarp();
-  }
-
-  // inverse z, stage 1 of task (r, j2): row r -> its z exchange (same warp).
-  __device__ static void zi1(T2 *buf, const T2 *ztw, int tid) {
-    const int j2 = tid & 7, r = tid >> 3;
-    T2 v[N1];
-    sfor<0, N1>([&](auto J1) { v[SPM_CI(J1)] = buf[r * M + SPM_CI(J1) * 8 + j2]; });
-    __syncwarp();
     Dft<+1, N1, T2>::run(v);
+    sfor<1, N1>([&](auto K1) {
+      constexpr int k1 = SPM_CI(K1);
+      v[k1] = cmulc(v[k1], ztw[k1 * 8 + j2]);
+    });
+    cluster_wait();  // the other CTAs are done reading this CTA's columns
     sfor<0, N1>([&](auto K1) {
       constexpr int k1 = SPM_CI(K1);
-      buf[zslot(r, j2, k1)] = (k1 == 0) ? v[k1] : cmulc(v[k1], ztw[k1 * 8 + j2]);
+      buf[zslot(r, j2, k1)] = v[k1];
     });
     __syncwarp();
   }
@@ -735,8 +731,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
       fence_proxy_async();
       issue(next);
     }
-    P::c2r_pre(buf, tw, tid, rank, cluster);
-    P::zi1(buf, ztw, tid);
+    P::c2r_zi1(buf, tw, ztw, tid, rank, cluster);
     P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
       const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
       const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, acc);
@@ -804,8 +799,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
     P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
       return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
     });
-    P::c2r_pre(buf, tw, tid, rank, cluster);
-    P::zi1(buf, ztw, tid);
+    P::c2r_zi1(buf, tw, ztw, tid, rank, cluster);
     if (stop) {
       P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
