@@ -87,16 +87,24 @@ const char *spm_status_str(int status);
  * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
  * inverse plane pass with the next step's forward one (phi stays on chip
  * between steps; the same bits as 0), 0 = three passes per step.
+ * knob "plane_xg" (0..3, plane_cps 2 and 3 only): the plane kernels of
+ * gradient chains exchange the x-plane between the CTAs of a cluster through
+ * distributed shared memory (0) or through per-CTA areas in global memory that
+ * stay resident in L2 (bit 1: the forward exchange, bit 2: the inverse one;
+ * the same bits either way). Nonzero allocates the areas (2 x resident CTAs x
+ * 16 N complex values).
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);
 /* Autotuner (no counterpart in the reference): times chains of `steps`
  * gradient steps on a scratch field for each candidate schedule (plane_cps
- * 1/2/3 with fused chains, plane_cps 2 without) and keeps the fastest in the
+ * 1/2/3 with fused chains, plane_cps 2 without, plane_xg 1/2/3 with plane_cps
+ * 2 and 3 on fused chains) and keeps the fastest in the
  * context; the choice is remembered per (device, N, precision), so later
  * contexts of the same kind take it without timing (FP32 twins of mixed flows
  * included). Synchronises; allocates two scratch fields while it runs. The
- * chosen knobs are returned in *plane_cps, *fuse_planes (may be NULL). */
+ * chosen knobs are returned in *plane_cps, *fuse_planes (may be NULL);
+ * spm_tune_get(ctx, "plane_xg") gives the exchange route. */
 int spm_autotune(spm_ctx *ctx, int steps, int *plane_cps, int *fuse_planes);
 const char *spm_last_error(void);
 /* Number of transform-kernel launches issued by this context so far. */

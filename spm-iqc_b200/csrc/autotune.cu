@@ -1,8 +1,10 @@
 // Autotuner for the transform schedule of a context (no counterpart in the
 // reference; FFTW's plan search plays this role there, My_FFT.cpp:49-97).
 // Candidates: the plane-pass variant (staged with one CTA per SM, direct loads
-// with two CTAs per SM, or three CTAs per SM with fewer registers per thread)
-// and whether gradient chains use the fused inverse -> forward plane pass.
+// with two CTAs per SM, or three CTAs per SM with fewer registers per thread),
+// whether gradient chains use the fused inverse -> forward plane pass, and
+// whether their plane kernels exchange through distributed shared memory or
+// through global areas resident in L2.
 // Each candidate runs a short chain of gradient steps on a scratch field with
 // CUDA events around it; the fastest is kept in the context and remembered per
 // (device, N, precision) for later contexts.
@@ -18,7 +20,10 @@
 namespace {
 
 std::mutex g_mu;
-std::map<std::tuple<int, int, int>, std::pair<int, int>> g_best;  // (device, N, prec) -> (plane_cps, fuse)
+struct Choice {
+  int plane_cps, fuse_planes, plane_xg;
+};
+std::map<std::tuple<int, int, int>, Choice> g_best;  // (device, N, prec) -> schedule
 
 // A smooth non-trivial field (a few cosines), so the timed steps do real work
 // and the flow does not stop on its first step.
@@ -34,27 +39,39 @@ template <class T> __global__ void fill_kernel(T *phi, int N) {
 }  // namespace
 
 // The remembered choice for (device, N, precision), if any.
-bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes) {
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg) {
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_best.find(std::make_tuple(device, N, prec));
   if (it == g_best.end()) return false;
-  *plane_cps = it->second.first;
-  *fuse_planes = it->second.second;
+  *plane_cps = it->second.plane_cps;
+  *fuse_planes = it->second.fuse_planes;
+  *plane_xg = it->second.plane_xg;
   return true;
 }
 
 extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_planes) {
   if (!c || steps < 2) return spm_fail(SPM_ERR_ARG, "bad argument (steps >= 2)");
   const auto key = std::make_tuple(c->device, c->N, c->prec);
+  auto finish = [&](const Choice &ch) {
+    c->plane_cps = ch.plane_cps;
+    c->fuse_planes = ch.fuse_planes;
+    c->plane_xg = ch.plane_xg;
+    if (!c->plane_xg && c->xg) {  // the exchange areas are not used by the chosen schedule
+      cudaStreamSynchronize(c->stream);
+      cudaFree(c->xg);
+      c->xg = nullptr;
+      c->xg_cap = 0;
+    }
+    if (plane_cps) *plane_cps = c->plane_cps;
+    if (fuse_planes) *fuse_planes = c->fuse_planes;
+    return spm_ensure_xg(c);
+  };
   {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_best.find(key);
     if (it != g_best.end()) {
-      c->plane_cps = it->second.first;
-      c->fuse_planes = it->second.second;
-      if (plane_cps) *plane_cps = c->plane_cps;
-      if (fuse_planes) *fuse_planes = c->fuse_planes;
-      return SPM_OK;
+      const Choice ch = it->second;
+      return finish(ch);
     }
   }
   void *phi = nullptr, *uh = nullptr;
@@ -64,14 +81,19 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   int rc = e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "autotune buffers");
-  const int saved_cps = c->plane_cps, saved_fuse = c->fuse_planes;
-  int best_cps = saved_cps, best_fuse = saved_fuse;
-  float best = 1e30f;
-  const int cands[][2] = {{2, 1}, {3, 1}, {1, 1}, {2, 0}};
-  for (const auto &cand : cands) {
+  const Choice saved = {c->plane_cps, c->fuse_planes, c->plane_xg};
+  Choice best = saved;
+  float best_ms = 1e30f;
+  // plane variant, fused plane pass, exchange routes of the gradient chains
+  const Choice cands[] = {{2, 1, 0}, {3, 1, 0}, {1, 1, 0}, {2, 0, 0}, {2, 1, spm::kXgFwd | spm::kXgInv},
+                          {3, 1, spm::kXgFwd | spm::kXgInv}, {2, 1, spm::kXgFwd}, {2, 1, spm::kXgInv}};
+  for (const Choice &cand : cands) {
     if (rc != SPM_OK) break;
-    c->plane_cps = cand[0];
-    c->fuse_planes = cand[1];
+    c->plane_cps = cand.plane_cps;
+    c->fuse_planes = cand.fuse_planes;
+    c->plane_xg = cand.plane_xg;
+    rc = spm_ensure_xg(c);
+    if (rc != SPM_OK) break;
     if (c->prec == SPM_FP64) fill_kernel<double><<<592, 256, 0, c->stream>>>((double *)phi, c->N);
     else fill_kernel<float><<<592, 256, 0, c->stream>>>((float *)phi, c->N);
     rc = spm_fft(c, phi, uh);
@@ -87,10 +109,9 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
       float ms = 0;
       if (rc == SPM_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < t) t = ms;
     }
-    if (rc == SPM_OK && t < best) {
-      best = t;
-      best_cps = cand[0];
-      best_fuse = cand[1];
+    if (rc == SPM_OK && t < best_ms) {
+      best_ms = t;
+      best = cand;
     }
   }
   if (e0) cudaEventDestroy(e0);
@@ -98,17 +119,12 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   cudaFree(phi);
   cudaFree(uh);
   if (rc != SPM_OK) {
-    c->plane_cps = saved_cps;
-    c->fuse_planes = saved_fuse;
+    finish(saved);
     return rc;
   }
-  c->plane_cps = best_cps;
-  c->fuse_planes = best_fuse;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_best[key] = {best_cps, best_fuse};
+    g_best[key] = best;
   }
-  if (plane_cps) *plane_cps = best_cps;
-  if (fuse_planes) *fuse_planes = best_fuse;
-  return SPM_OK;
+  return finish(best);
 }

@@ -27,6 +27,11 @@ namespace spm {
 constexpr int kThreads = 256;   // threads per CTA in every transform kernel
 constexpr int kRows = 32;       // z-lines (rows of an x-plane) per CTA, plane kernels
 constexpr int kCols = 16;       // y-lines (spectral columns) per CTA, plane kernels
+// Exchange routes of the plane kernels (template XG): the forward exchange
+// (R2C rows -> forward y columns) and the inverse one (inverse y columns ->
+// C2R rows) go through distributed shared memory, or, with these bits, through
+// per-CTA global areas that stay resident in L2.
+constexpr int kXgFwd = 1, kXgInv = 2;
 constexpr int kMaxBatch = 16;   // fields per launch
 constexpr int kScal = 16;       // scalars per field in the scalar block
 constexpr int kRedMax = 8;      // reduction slots per field and CTA
@@ -376,6 +381,8 @@ struct KParams {
   double *stats;        // grad-flow per-step records (or null)
   const double4 *gtab;  // per K^2 = Kx^2+Ky^2+Kz^2: {G, 1/(1+dt G), 1/(G+|Tau|+0.02), 1/(1+G)}
   int *err;             // set when a bounded wait timed out
+  void *xg;             // plane kernels with XG: global exchange areas, 2 x xg_cap CTAs x PLANE_UNITS complex
+  int xg_cap;
   int nb;
 };
 

@@ -60,6 +60,22 @@ __device__ __forceinline__ bool flow_stopped(const KParams &p) {
   return p.flow != nullptr && *((volatile const int *)p.flow + FW_GO) == 0;
 }
 
+// This CTA's global exchange area (e = 0: inverse exchange, 1: forward) and
+// that of rank 0 of its cluster (the cluster's CTAs are consecutive in x).
+template <int N, class T> struct XgAreas {
+  c2<T> *own[2] = {nullptr, nullptr};
+  const c2<T> *first[2] = {nullptr, nullptr};
+  __device__ XgAreas(const KParams &p, int rank) {
+    if (p.xg == nullptr) return;
+    constexpr size_t U = Geo<N>::PLANE_UNITS;
+    c2<T> *xg = reinterpret_cast<c2<T> *>(p.xg);
+    for (int e = 0; e < 2; e++) {
+      own[e] = xg + ((size_t)e * p.xg_cap + blockIdx.x) * U;
+      first[e] = xg + ((size_t)e * p.xg_cap + blockIdx.x - rank) * U;
+    }
+  }
+};
+
 __device__ __forceinline__ void report_error(const KParams &p, int s_err) {
   if (s_err && p.err && threadIdx.x == 0) atomicExch(p.err, 1);
 }
@@ -98,8 +114,10 @@ template <int N, class T> struct Plane {
   // forward z, stage 2 (8-point DFTs over j2 -> k = k1 + N1*k2) and the
   // real-to-complex post-processing of the packed lines (pairs q, M-q), each
   // warp on its own rows. Ends with a cluster barrier: the rows [r][M] are
-  // then ready for remote reads.
-  __device__ static void zf2_post(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster) {
+  // then ready for remote reads, in buf or (XG) in the CTA's global exchange
+  // area gx.
+  template <bool XG = false>
+  __device__ static void zf2_post(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, T2 *gx = nullptr) {
     const int warp = tid >> 5, lane = tid & 31;
     {
       constexpr int NT = RPW * N1;  // tasks (r, k1) of this warp
@@ -131,22 +149,23 @@ template <int N, class T> struct Plane {
       constexpr int NT = RPW * (M / 2);
       for (int task = lane; task < NT; task += 32) {
         const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
-        T2 *Z = buf + r * M;
+        const T2 *Z = buf + r * M;
+        T2 *O = (XG ? gx : buf) + r * M;
         if (q == 0) {
           const T2 z0 = Z[0];
-          Z[0] = T2{z0.x + z0.y, z0.x - z0.y};  // X_0 + i X_{N/2}
           const T2 a = Z[M / 2];
           const T2 e = {a.x, (T)0};            // (a + conj a)/2
           const T2 o = {a.y, (T)0};            // (a - conj a)/(2i)
-          Z[M / 2] = cadd(e, cmul(tw[M / 2], o));
+          O[0] = T2{z0.x + z0.y, z0.x - z0.y};  // X_0 + i X_{N/2}
+          O[M / 2] = cadd(e, cmul(tw[M / 2], o));
         } else {
           const T2 a = Z[q], c = Z[M - q];
           const T2 e1 = {(T)0.5 * (a.x + c.x), (T)0.5 * (a.y - c.y)};  // (Z_q + conj Z_{M-q})/2
           const T2 o1 = {(T)0.5 * (a.y + c.y), (T)0.5 * (c.x - a.x)};  // (Z_q - conj Z_{M-q})/(2i)
           const T2 e2 = {e1.x, -e1.y};
           const T2 o2 = {o1.x, -o1.y};
-          Z[q] = cadd(e1, cmul(tw[q], o1));
-          Z[M - q] = cadd(e2, cmul(tw[M - q], o2));
+          O[q] = cadd(e1, cmul(tw[q], o1));
+          O[M - q] = cadd(e2, cmul(tw[M - q], o2));
         }
       }
     }
@@ -155,9 +174,14 @@ template <int N, class T> struct Plane {
 
   // forward y over this CTA's 16 columns: gather element y = 16*j1 + j2 of
   // column c from the CTA holding row y, radix-M1 DFT, exchange, radix-16
-  // DFT, store the spectral column into dst[plane][ky][M].
+  // DFT, store the spectral column into dst[plane][ky][M]. With XG the rows
+  // come from the global exchange areas of the cluster's CTAs (gp = the area
+  // of rank 0; rank k's at gp + k * PLANE_UNITS), which stay untouched until
+  // every CTA has passed the next plane's first cluster barrier, so no
+  // "done reading" barrier is needed.
+  template <bool XG = false>
   __device__ static void yf(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster, T2 *dst,
-                            int plane) {
+                            int plane, const T2 *gp = nullptr) {
     {
       const int c = tid & 15, j2 = tid >> 4;
       const int col = rank * kCols + c;
@@ -165,18 +189,22 @@ template <int N, class T> struct Plane {
       sfor<0, M1>([&](auto J1) {
         constexpr int j1 = SPM_CI(J1);
         const int y = 16 * j1 + j2;
-        const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
-        v[j1] = rem[(y & 31) * M + col];
+        if constexpr (XG) {
+          v[j1] = __ldcg(gp + (size_t)(y >> 5) * G::PLANE_UNITS + (y & 31) * M + col);
+        } else {
+          const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
+          v[j1] = rem[(y & 31) * M + col];
+        }
       });
       Dft<-1, M1, T2>::run(v);  // consumes every gathered value
       // done reading the other CTAs' rows: they may overwrite them after the
       // wait, which comes after the twiddles
-      cluster_arrive_relaxed();
+      if constexpr (!XG) cluster_arrive_relaxed();
       sfor<1, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
         v[k1] = cmul(v[k1], tw[j2 * k1]);
       });
-      cluster_wait();
+      if constexpr (!XG) cluster_wait();
       sfor<0, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
         buf[k1 * 256 + j2 * 16 + c] = v[k1];
@@ -203,9 +231,10 @@ template <int N, class T> struct Plane {
   __device__ static int ycol(int y, int c) { return (y % M1) * 256 + (y / M1) * 16 + c; }
 
   // inverse y over this CTA's 16 columns; ld(ky, c) returns the input value.
-  // Leaves y-line values at ycol(y, c) in buf and ends with a cluster barrier.
-  template <class LD>
-  __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld) {
+  // Leaves y-line values at ycol(y, c) in buf (or, XG, in the CTA's global
+  // exchange area gx) and ends with a cluster barrier.
+  template <bool XG = false, class LD>
+  __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld, T2 *gx = nullptr) {
     {
       const int c = tid & 15, j2 = tid >> 4;
       T2 v[M1];
@@ -227,7 +256,7 @@ template <int N, class T> struct Plane {
       for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
       Dft<+1, 16, T2>::run(u);
 #pragma unroll
-      for (int k2 = 0; k2 < 16; k2++) buf[k1 * 256 + k2 * 16 + c] = u[k2];  // = ycol(k1 + M1*k2, c)
+      for (int k2 = 0; k2 < 16; k2++) (XG ? gx : buf)[k1 * 256 + k2 * 16 + c] = u[k2];  // = ycol(k1 + M1*k2, c)
     }
     cluster.sync();
   }
@@ -241,20 +270,27 @@ template <int N, class T> struct Plane {
   // pairs q = 0 with M/2; lanes 0 and 4 are their own partners). The "done
   // reading" arrive follows the last use of a gathered value and its wait
   // comes only before the stores into the row, so the radix-N1 DFT runs in
-  // between. Ends with the z exchange of each row written (same warp).
+  // between. Ends with the z exchange of each row written (same warp). With
+  // XG the columns come from the global exchange areas of the cluster's CTAs
+  // (gp as in yf) and buf is free at once.
+  template <bool XG = false>
   __device__ static void c2r_zi1(T2 *buf, const T2 *tw, const T2 *ztw, int tid, int rank,
-                                 cg::cluster_group &cluster) {
+                                 cg::cluster_group &cluster, const T2 *gp = nullptr) {
     constexpr int H = N1 / 2;
     static_assert(N1 % 2 == 0, "pairs");
     const int j2 = tid & 7, r = tid >> 3, lane = tid & 31;
     const int y = rank * kRows + r;
+    auto col = [&](int q) -> T2 {  // X_q of row y from its column owner
+      if constexpr (XG) return __ldcg(gp + (size_t)(q / kCols) * G::PLANE_UNITS + ycol(y, q % kCols));
+      else return cluster.map_shared_rank(buf, (unsigned)(q / kCols))[ycol(y, q % kCols)];
+    };
     T2 v[N1], w[H];
 #pragma unroll
     for (int j = 0; j < H; j++) {
       const int q = 8 * j + j2;
       if (q == 0) {
-        const T2 P = cluster.map_shared_rank(buf, 0u)[ycol(y, 0)];
-        const T2 a = cluster.map_shared_rank(buf, (unsigned)((M / 2) / kCols))[ycol(y, (M / 2) % kCols)];
+        const T2 P = col(0);
+        const T2 a = col(M / 2);
         // Z_0 = (X0 + XM) + i (X0 - XM) from the packed value P = X0 + i XM
         v[0] = T2{P.x + P.y, P.x - P.y};
         // Z_{M/2} = (a + conj a) + i w^{-M/2} (a - conj a)
@@ -262,8 +298,8 @@ template <int N, class T> struct Plane {
         const T2 o = {(T)0, a.y + a.y};
         w[0] = cadd(e, mul_di<+1>(cmulc(o, tw[M / 2])));
       } else {
-        const T2 a = cluster.map_shared_rank(buf, (unsigned)(q / kCols))[ycol(y, q % kCols)];
-        const T2 c = cluster.map_shared_rank(buf, (unsigned)((M - q) / kCols))[ycol(y, (M - q) % kCols)];
+        const T2 a = col(q);
+        const T2 c = col(M - q);
         // Z_q = (X_q + conj X_{M-q}) + i w^{-q} (X_q - conj X_{M-q})
         const T2 e1 = {a.x + c.x, a.y - c.y}, d1 = {a.x - c.x, a.y + c.y};
         const T2 e2 = {c.x + a.x, c.y - a.y}, d2 = {c.x - a.x, c.y + a.y};
@@ -272,7 +308,7 @@ template <int N, class T> struct Plane {
       }
     }
     // every gathered value is consumed: done reading the column owners
-    cluster_arrive_relaxed();
+    if constexpr (!XG) cluster_arrive_relaxed();
     const int src = (lane & ~7) | ((8 - j2) & 7);
 #pragma unroll
     for (int j = 0; j < H; j++) {
@@ -286,7 +322,7 @@ template <int N, class T> struct Plane {
       constexpr int k1 = SPM_CI(K1);
       v[k1] = cmulc(v[k1], ztw[k1 * 8 + j2]);
     });
-    cluster_wait();  // the other CTAs are done reading this CTA's columns
+    if constexpr (!XG) cluster_wait();  // the other CTAs are done reading this CTA's columns
     sfor<0, N1>([&](auto K1) {
       constexpr int k1 = SPM_CI(K1);
       buf[zslot(r, j2, k1)] = v[k1];
@@ -358,7 +394,7 @@ template <int N, class T> __device__ __forceinline__ void plane_twiddles(const K
 // CPS = CTAs per SM the variant is built for: 1 stages the next plane's rows
 // in shared memory with a bulk copy; 2 has no stage (half the shared memory,
 // so two CTAs share an SM) and loads its rows straight from global memory.
-template <int N, class T, class Pro, int CPS>
+template <int N, class T, class Pro, int CPS, int XG = 0>
 __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
@@ -379,6 +415,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
+  const XgAreas<N, T> xa(p, rank);
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   const T *src = reinterpret_cast<const T *>(p.in[b]);
   T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
@@ -424,8 +461,11 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       fence_proxy_async();
       issue(next);
     }
-    P::zf2_post(buf, tw, tid, cluster);
-    P::yf(buf, tw, tid, rank, cluster, dst, plane);
+    // one cluster barrier per plane here: the two areas alternate, so a CTA
+    // rewrites an area only after every CTA has passed the barrier that
+    // follows the last reads of it
+    P::template zf2_post<(XG & kXgFwd) != 0>(buf, tw, tid, cluster, xa.own[it & 1]);
+    P::template yf<(XG & kXgFwd) != 0>(buf, tw, tid, rank, cluster, dst, plane, xa.first[it & 1]);
     __syncthreads();
   }
   report_error(p, s_err);
@@ -677,7 +717,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
 //      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
 // CPS as for plane_fwd: 1 stages the next plane's columns with a tensor copy,
 // 2 loads them straight from global memory (two CTAs per SM).
-template <int N, class T, class Epi, int CPS>
+template <int N, class T, class Epi, int CPS, int XG = 0>
 __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
@@ -698,6 +738,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
+  const XgAreas<N, T> xa(p, rank);
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   auto issue = [&](int plane) {  // thread 0: one tensor box (this CTA's 16 columns x all ky)
     mbar_expect_tx(bar, (unsigned)(N * 16 * sizeof(T2)));
@@ -724,14 +765,17 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     // next plane's columns towards L2 while this one is transformed
     if (!STAGED && next < N && tid < N)
       prefetch_l2(gsrc + ((size_t)next * N + tid) * M + rank * kCols, kCols * sizeof(T2));
-    P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
-      return STAGED ? stage[ky * 16 + c] : __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
-    });
+    P::template yi<(XG & kXgInv) != 0>(
+        buf, tw, tid, cluster,
+        [&](int ky, int c) -> T2 {
+          return STAGED ? stage[ky * 16 + c] : __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
+        },
+        xa.own[it & 1]);  // alternating areas, as in plane_fwd
     if (STAGED && tid == 0 && next < N) {
       fence_proxy_async();
       issue(next);
     }
-    P::c2r_zi1(buf, tw, ztw, tid, rank, cluster);
+    P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[it & 1]);
     P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
       const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
       const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, acc);
@@ -758,7 +802,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
 // plane_inv, so the real field crosses HBM once per chain instead of twice per
 // step. Direct loads; CPS (2 or 3) CTAs per SM, the layout of plane_fwd's
 // direct variant.
-template <int N, class T, class Epi, class Pro, int CPS>
+template <int N, class T, class Epi, class Pro, int CPS, int XG = 0>
 __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
@@ -780,6 +824,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
+  const XgAreas<N, T> xa(p, rank);
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   plane_twiddles<N, T>(p, tw, ztw);
   double acc_e[NE > 0 ? NE : 1], acc_p[NP > 0 ? NP : 1];
@@ -796,15 +841,19 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
     // next plane's columns towards L2 while this one is transformed
     if (plane + ncl < N && tid < N)
       prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + tid) * M + rank * kCols, kCols * sizeof(T2));
-    P::yi(buf, tw, tid, cluster, [&](int ky, int c) -> T2 {
-      return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
-    });
-    P::c2r_zi1(buf, tw, ztw, tid, rank, cluster);
+    P::template yi<(XG & kXgInv) != 0>(
+        buf, tw, tid, cluster,
+        [&](int ky, int c) -> T2 { return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c); },
+        xa.own[0]);
+    P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[0]);
     if (stop) {
       P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
         reinterpret_cast<T2 *>(phi + rowoff)[j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
       });
+      // no forward exchange on this path: its barrier keeps the inverse areas
+      // of this plane from being rewritten while a peer still reads them
+      if constexpr ((XG & kXgInv) != 0) cluster.sync();
     } else {
       // phi rows [r][M] in buf (each warp writes and then reads its own rows)
       P::template zi2<true>(buf, tid, [&](int r, int j, T2 z) {
@@ -825,8 +874,8 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
         P::zf1_store(buf, ztw, v, r, j2);
       }
       __syncwarp();
-      P::zf2_post(buf, tw, tid, cluster);
-      P::yf(buf, tw, tid, rank, cluster, dst, plane);
+      P::template zf2_post<(XG & kXgFwd) != 0>(buf, tw, tid, cluster, xa.own[1]);
+      P::template yf<(XG & kXgFwd) != 0>(buf, tw, tid, rank, cluster, dst, plane, xa.first[1]);
     }
     __syncthreads();
   }

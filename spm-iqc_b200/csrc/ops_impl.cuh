@@ -4,6 +4,7 @@
 #pragma once
 
 #include <atomic>
+#include <type_traits>
 
 #include "../../include/spmiqc.h"
 #include "blas1.cuh"
@@ -33,7 +34,7 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
 // Persistent cluster launch: as many clusters as can be resident at once
 // (queried once per kernel and device), at most one per x-plane.
 template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p,
-                                                               int nb, const char *what) {
+                                                               int nb, const char *what, bool xg = false) {
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, what);
   cudaLaunchConfig_t cfg = {};
@@ -61,14 +62,37 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
     ncl[dev].store(nc, std::memory_order_relaxed);
   }
   cfg.gridDim = dim3(Geo<N>::CL * nc, nb, 1);
+  // a kernel exchanging through global areas needs one per CTA (nb == 1)
+  if (xg && (!p.xg || nb != 1 || Geo<N>::CL * nc > p.xg_cap))
+    return spm_fail(SPM_ERR_STATE, "plane exchange areas missing or too small");
   c->launches++;
   e = cudaLaunchKernelEx(&cfg, kern, p);
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, what);
 }
 
-// The plane kernels come in two variants (c->plane_cps): 1 = staged, one CTA
-// per SM; 2 = direct loads, two CTAs per SM.
+// Gradient-chain kernels (the nonlinear prologue and the flow epilogue) may
+// exchange through the global areas (c->plane_xg, autotuned); other chains
+// (batched Hv, preconditioner, ...) always use distributed shared memory.
+template <class X> struct XgOk : std::false_type {};
+template <class T> struct XgOk<ProGrad<T>> : std::true_type {};
+template <class T> struct XgOk<EpiFlow<T>> : std::true_type {};
+static inline int xg_bits(const spm_ctx *c, int nb) { return (c->xg && nb == 1 && c->plane_cps >= 2) ? c->plane_xg : 0; }
+
+// The plane kernels come in three variants (c->plane_cps): 1 = staged, one
+// CTA per SM; 2 = direct loads, two CTAs per SM; 3 = direct, three CTAs per SM.
 template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
+  if constexpr (XgOk<Pro>::value) {
+    if (xg_bits(c, nb) & kXgFwd) {
+      if (c->plane_cps == 3) {
+        struct Tag3x {};
+        return launch_cluster<Tag3x, N>(c, plane_fwd_kernel<N, T, Pro, 3, kXgFwd>, plane_smem<N, T, 3>(), p, nb,
+                                        "plane_fwd", true);
+      }
+      struct Tag2x {};
+      return launch_cluster<Tag2x, N>(c, plane_fwd_kernel<N, T, Pro, 2, kXgFwd>, plane_smem<N, T, 2>(), p, nb,
+                                      "plane_fwd", true);
+    }
+  }
   if (c->plane_cps == 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_fwd_kernel<N, T, Pro, 3>, plane_smem<N, T, 3>(), p, nb, "plane_fwd");
@@ -81,6 +105,18 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
   return launch_cluster<Tag1, N>(c, plane_fwd_kernel<N, T, Pro, 1>, plane_smem<N, T, 1>(), p, nb, "plane_fwd");
 }
 template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p0, int nb) {
+  if constexpr (XgOk<Epi>::value) {
+    if (xg_bits(c, nb) & kXgInv) {
+      if (c->plane_cps == 3) {
+        struct Tag3x {};
+        return launch_cluster<Tag3x, N>(c, plane_inv_kernel<N, T, Epi, 3, kXgInv>, plane_smem<N, T, 3>(), p0, nb,
+                                        "plane_inv", true);
+      }
+      struct Tag2x {};
+      return launch_cluster<Tag2x, N>(c, plane_inv_kernel<N, T, Epi, 2, kXgInv>, plane_smem<N, T, 2>(), p0, nb,
+                                      "plane_inv", true);
+    }
+  }
   if (c->plane_cps == 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_inv_kernel<N, T, Epi, 3>, plane_smem<N, T, 3>(), p0, nb, "plane_inv");
@@ -95,16 +131,28 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
   return launch_cluster<Tag1, N>(c, plane_inv_kernel<N, T, Epi, 1>, plane_smem<N, T, 1>(), p, nb, "plane_inv");
 }
 // The fused inverse -> forward plane pass (direct loads; two CTAs per SM, or
-// three with plane_cps = 3).
-template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
+// three with plane_cps = 3), with the exchange routes XG.
+template <int N, class T, class Epi, class Pro, int XG>
+static int plane_inv_fwd_xg(spm_ctx *c, const KParams &p, int nb) {
   if (c->plane_cps == 3) {
     struct Tag3 {};
-    return launch_cluster<Tag3, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 3>, plane_smem<N, T, 3>(), p, nb,
-                                   "plane_inv_fwd");
+    return launch_cluster<Tag3, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 3, XG>, plane_smem<N, T, 3>(), p, nb,
+                                   "plane_inv_fwd", XG != 0);
   }
   struct Tag2 {};
-  return launch_cluster<Tag2, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 2>, plane_smem<N, T, 2>(), p, nb,
-                                 "plane_inv_fwd");
+  return launch_cluster<Tag2, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 2, XG>, plane_smem<N, T, 2>(), p, nb,
+                                 "plane_inv_fwd", XG != 0);
+}
+template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
+  if constexpr (XgOk<Pro>::value && XgOk<Epi>::value) {
+    switch (xg_bits(c, nb)) {
+      case kXgFwd: return plane_inv_fwd_xg<N, T, Epi, Pro, kXgFwd>(c, p, nb);
+      case kXgInv: return plane_inv_fwd_xg<N, T, Epi, Pro, kXgInv>(c, p, nb);
+      case kXgFwd | kXgInv: return plane_inv_fwd_xg<N, T, Epi, Pro, kXgFwd | kXgInv>(c, p, nb);
+      default: break;
+    }
+  }
+  return plane_inv_fwd_xg<N, T, Epi, Pro, 0>(c, p, nb);
 }
 // Persistent pencil launch: resident CTAs (queried once), at most one per tile.
 template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p0, int nb) {

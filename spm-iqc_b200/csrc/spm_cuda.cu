@@ -84,10 +84,38 @@ KParams spm_params(const spm_ctx *c) {
   p.flow = c->gate;
   p.gtab = reinterpret_cast<const double4 *>(c->gtab);
   p.err = c->flow + FW_ERR;
+  p.xg = c->xg;
+  p.xg_cap = c->xg_cap;
   return p;
 }
 
+// One area per resident CTA of a plane kernel and exchange: at most
+// min(SMs x CTAs per SM, N x CL) CTAs, the CTAs per SM bounded by the plane
+// kernels' shared memory and 8 blocks of 256 threads.
+int spm_ensure_xg(spm_ctx *c) {
+  if (!c->plane_xg || c->xg) return SPM_OK;
+  int sms = 0, smem_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "device attributes");
+  const size_t cplx = c->prec == SPM_FP64 ? 16 : 8;
+  const size_t units = 16 * (size_t)c->N;  // PLANE_UNITS
+  const size_t smem = cplx * (c->N + c->N / 2 + units) + 16 + 8 * 32 * spm::kRedMax + 128 + 1024;
+  int per_sm = (int)(smem_sm / smem);
+  per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
+  const int most = c->N * (c->N / spm::kRows);
+  const int cap = sms * per_sm < most ? sms * per_sm : most;
+  e = cudaMalloc(&c->xg, 2 * (size_t)cap * units * cplx);
+  if (e != cudaSuccess) {
+    c->xg = nullptr;
+    return spm_fail_cuda(e, "plane exchange areas");
+  }
+  c->xg_cap = cap;
+  return SPM_OK;
+}
+
 int spm_ensure_scratch(spm_ctx *c, int nb) {
+  SPM_TRY(spm_ensure_xg(c));
   if (nb <= c->scratch_cap) return SPM_OK;
   if (c->bufA) cudaFree(c->bufA);
   if (c->bufB) cudaFree(c->bufB);
@@ -292,6 +320,7 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
   cudaFree(c->stats);
   cudaFree(c->bufA);
   cudaFree(c->bufB);
+  cudaFree(c->xg);
   cudaFree(c->host_phi);
   cudaFree(c->host_uhat);
   if (c->host_scal) cudaFreeHost(c->host_scal);
@@ -312,6 +341,11 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->fuse_planes = value;
     return SPM_OK;
   }
+  if (std::strcmp(knob, "plane_xg") == 0) {
+    if (value < 0 || value > 3) return spm_fail(SPM_ERR_ARG, "plane_xg must be 0..3");
+    c->plane_xg = value;
+    return spm_ensure_xg(c);
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
@@ -319,6 +353,7 @@ extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (!c || !knob) return -1;
   if (std::strcmp(knob, "plane_cps") == 0) return c->plane_cps;
   if (std::strcmp(knob, "fuse_planes") == 0) return c->fuse_planes;
+  if (std::strcmp(knob, "plane_xg") == 0) return c->plane_xg;
   return -1;
 }
 
@@ -488,9 +523,10 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->cancel = c->cancel;
   c->twin->plane_cps = c->plane_cps;
   c->twin->fuse_planes = c->fuse_planes;
+  c->twin->plane_xg = c->plane_xg;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
-  spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes);
-  return SPM_OK;
+  spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg);
+  return spm_ensure_xg(c->twin);
 }
 
 // Mixed precision: FP32 transforms with FP64 reductions until ||grad F|| <=

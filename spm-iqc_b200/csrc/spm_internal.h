@@ -50,6 +50,9 @@ struct spm_ctx {
   std::vector<TmEntry> tmaps;   // tensor-map cache (most recent last)
   int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
   int fuse_planes = 1;          // gradient chains use the fused inverse -> forward plane pass
+  int plane_xg = 0;             // gradient-chain plane kernels: exchanges through L2 (spm::kXgFwd | kXgInv bits)
+  void *xg = nullptr;           // their global exchange areas (2 x xg_cap CTAs x 16 N complex)
+  int xg_cap = 0;
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
   const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)
@@ -61,6 +64,8 @@ int spm_fail(int status, const char *what);
 int spm_fail_cuda(cudaError_t e, const char *what);
 spm::KParams spm_params(const spm_ctx *c);
 int spm_ensure_scratch(spm_ctx *c, int nb);
+// Allocates the global exchange areas when c->plane_xg asks for them.
+int spm_ensure_xg(spm_ctx *c);
 char *spm_bufA(spm_ctx *c, int b);
 char *spm_bufB(spm_ctx *c, int b);
 int spm_read_scal(spm_ctx *c, int nb);
@@ -74,5 +79,5 @@ void spm_free_extra(spm_ctx *c);
 // to the context's stream, cancel flag and tuning.
 int spm_ensure_twin(spm_ctx *c);
 // The autotuner's remembered choice for (device, N, precision), if any.
-bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes);
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg);
 const struct OpsTable *spm_table_of(const spm_ctx *c);

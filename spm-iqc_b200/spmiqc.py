@@ -243,6 +243,12 @@ class SpmContext:
         check(f(self.h, int(steps), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def tuning(self) -> dict:
+        """The current values of the tuning knobs (spm_tune_get)."""
+        f = lib().spm_tune_get
+        f.argtypes = [_vp, ctypes.c_char_p]
+        return {k: int(f(self.h, k.encode())) for k in ("plane_cps", "fuse_planes", "plane_xg")}
+
     def ngrad_cam(self, phi, grad=None):
         grad = self.field() if grad is None else grad
         nrm = ctypes.c_double()

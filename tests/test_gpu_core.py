@@ -134,6 +134,33 @@ def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
     assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
 
 
+@pytest.mark.parametrize("N,prec", [(64, "fp64"), (256, "fp64"), (128, "fp32")])
+def test_exchange_routes_are_bit_identical(spm, cuda, N, prec):
+    """Gradient chains whose plane kernels exchange through global areas in L2
+    (plane_xg 1, 2, 3; plane_cps 2 and 3) give the same fields as exchanges
+    through distributed shared memory, and records equal to rounding."""
+    phi = npo.uniform_field(N, 12)
+    dt = np.float64 if prec == "fp64" else np.float32
+    out = []
+    for cps, xg in ((2, 0), (2, 1), (2, 2), (2, 3), (3, 3)):
+        e = spm.SpmContext(N, Tau=-0.02, precision=prec)
+        e.tune("plane_cps", cps)
+        e.tune("plane_xg", xg)
+        assert e.tuning()["plane_xg"] == xg
+        p = t(cuda, phi.astype(dt))
+        u = e.my_fft(p)
+        st = e.get_min_u_F(p, u, 23)
+        mid = (p.cpu().numpy(), u.cpu().numpy())
+        # then a flow that stops inside a chain (the fused pass's stopping path)
+        st2 = e.get_min_u_F(p, u, 3000, tol_grad=float(st[-1, 2]) * 0.5)
+        out.append((st, mid, len(st2), p.cpu().numpy(), u.cpu().numpy()))
+    for st, mid, n2, p, u in out[1:]:
+        assert np.array_equal(mid[0], out[0][1][0]) and np.array_equal(mid[1], out[0][1][1])
+        assert n2 == out[0][2] < 3000
+        assert np.array_equal(p, out[0][3]) and np.array_equal(u, out[0][4])
+        assert rel(st, out[0][0]) < 1e-12
+
+
 def test_autotune_picks_a_schedule_and_keeps_results(spm, cuda):
     """The autotuner returns one of its candidates, remembers it for the next
     context of the same kind, and every schedule gives the same fields (the
@@ -145,6 +172,7 @@ def test_autotune_picks_a_schedule_and_keeps_results(spm, cuda):
     assert cps in (1, 2, 3) and fuse in (0, 1)
     d = spm.SpmContext(N)
     assert d.autotune(10) == (cps, fuse)
+    assert d.tuning() == c.tuning() and c.tuning()["plane_xg"] in (0, 1, 2, 3)
     phi = npo.uniform_field(N, 8)
     out = []
     for k_cps, k_fuse in ((1, 1), (2, 1), (3, 1), (2, 0)):
