@@ -379,6 +379,9 @@ def main():
     ap.add_argument("--only-flow", action="store_true",
                     help="run only the warm-up and timed gradient steps (used for ncu captures)")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs mixed time-to-tolerance leg")
+    ap.add_argument("--schedule", default=None,
+                    help="plane_cps,fuse_planes,plane_xg for the FP64 context instead of the autotuner's choice "
+                         "(fixed kernel variants for ncu captures)")
     ap.add_argument("--serve", action="store_true", help="run the serving workload instead (one JSON line)")
     ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--serve-slots", type=int, default=6)
@@ -409,9 +412,16 @@ def main():
     ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp64", stream=stream.cuda_stream)
     # schedule choice by the autotuner, outside the timed region (FP32 too, for
     # the FP32 leg and the FP32 twin of the mixed flow)
-    sched64 = ctx.autotune(20)
+    if args.schedule:
+        for knob, v in zip(("plane_cps", "fuse_planes", "plane_xg"), args.schedule.split(",")):
+            ctx.tune(knob, int(v))
+    else:
+        ctx.autotune(20)
+    sched64 = ctx.tuning()
     _c32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
-    sched32 = _c32.autotune(20)
+    if not args.schedule:
+        _c32.autotune(20)
+    sched32 = _c32.tuning()
     _c32.close()
     phi_h = initial_field(1 + rank)
     phi = torch.from_numpy(phi_h).cuda()
@@ -508,7 +518,8 @@ def main():
 
     # FP32 bulk (same workload, FP32 transforms, FP64 reductions)
     ctx32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
-    ctx32.autotune(20)  # the remembered FP32 choice
+    if not args.schedule:
+        ctx32.autotune(20)  # the remembered FP32 choice
     phi32 = torch.from_numpy(phi_h.astype(np.float32)).cuda()
     uh32 = ctx32.my_fft(phi32)
     run_steps(args.warmup, phi32, uh32, ctx32)
@@ -587,8 +598,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "N": N, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (0.81 GB of fields through HBM per step)",
-                       "schedule_fp64": {"plane_cps": sched64[0], "fuse_planes": sched64[1]},
-                       "schedule_fp32": {"plane_cps": sched32[0], "fuse_planes": sched32[1]}},
+                       "schedule_fp64": sched64, "schedule_fp32": sched32},
             "p50_ms": p50, "p99_ms": p99,
             "hv_per_s": hv_per_s, "fp32_steps_per_s": fp32_value, "precision": precision,
             "kernels_ms": dict(zip(names, kms)),

@@ -297,6 +297,54 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
 __device__ __forceinline__ void prefetch_l2(const void *src, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
+// Accesses of the plane kernels' global exchange areas with an L2
+// "evict last" policy, so the areas (a few tens of MB, rewritten every plane)
+// stay in L2 while the streamed fields pass through it; the loads bypass L1
+// (ld.global.cg: other SMs rewrite the areas between planes).
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void st_keep(double2 *p, double2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_keep(float2 *p, float2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ double2 ld_keep(const double2 *p, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float2 ld_keep(const float2 *p, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+
+// Streamed field data (read or written once per pass) with an L2 "evict
+// first" policy, so it does not push the exchange areas out of L2.
+__device__ __forceinline__ uint64_t l2_stream_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double2 ld_stream(const double2 *p, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float2 ld_stream(const float2 *p, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_stream(double2 *p, double2 v, uint64_t pol) { st_keep(p, v, pol); }
+__device__ __forceinline__ void st_stream(float2 *p, float2 v, uint64_t pol) { st_keep(p, v, pol); }
+
 // Cluster barrier halves. arrive_relaxed orders nothing: use it where a CTA
 // only signals that it has finished READING other CTAs' shared memory (every
 // loaded value already consumed by an instruction before it), so that they

@@ -147,25 +147,30 @@ template <int N, class T> struct Plane {
     __syncwarp();
     {
       constexpr int NT = RPW * (M / 2);
+      const uint64_t pol = XG ? l2_keep_policy() : 0;
       for (int task = lane; task < NT; task += 32) {
         const int r = RPW * warp + task / (M / 2), q = task % (M / 2);
         const T2 *Z = buf + r * M;
         T2 *O = (XG ? gx : buf) + r * M;
+        auto put = [&](int i, T2 v) {
+          if constexpr (XG) st_keep(O + i, v, pol);
+          else O[i] = v;
+        };
         if (q == 0) {
           const T2 z0 = Z[0];
           const T2 a = Z[M / 2];
           const T2 e = {a.x, (T)0};            // (a + conj a)/2
           const T2 o = {a.y, (T)0};            // (a - conj a)/(2i)
-          O[0] = T2{z0.x + z0.y, z0.x - z0.y};  // X_0 + i X_{N/2}
-          O[M / 2] = cadd(e, cmul(tw[M / 2], o));
+          put(0, T2{z0.x + z0.y, z0.x - z0.y});  // X_0 + i X_{N/2}
+          put(M / 2, cadd(e, cmul(tw[M / 2], o)));
         } else {
           const T2 a = Z[q], c = Z[M - q];
           const T2 e1 = {(T)0.5 * (a.x + c.x), (T)0.5 * (a.y - c.y)};  // (Z_q + conj Z_{M-q})/2
           const T2 o1 = {(T)0.5 * (a.y + c.y), (T)0.5 * (c.x - a.x)};  // (Z_q - conj Z_{M-q})/(2i)
           const T2 e2 = {e1.x, -e1.y};
           const T2 o2 = {o1.x, -o1.y};
-          O[q] = cadd(e1, cmul(tw[q], o1));
-          O[M - q] = cadd(e2, cmul(tw[M - q], o2));
+          put(q, cadd(e1, cmul(tw[q], o1)));
+          put(M - q, cadd(e2, cmul(tw[M - q], o2)));
         }
       }
     }
@@ -185,12 +190,13 @@ template <int N, class T> struct Plane {
     {
       const int c = tid & 15, j2 = tid >> 4;
       const int col = rank * kCols + c;
+      const uint64_t pol = XG ? l2_keep_policy() : 0;
       T2 v[M1];
       sfor<0, M1>([&](auto J1) {
         constexpr int j1 = SPM_CI(J1);
         const int y = 16 * j1 + j2;
         if constexpr (XG) {
-          v[j1] = __ldcg(gp + (size_t)(y >> 5) * G::PLANE_UNITS + (y & 31) * M + col);
+          v[j1] = ld_keep(gp + (size_t)(y >> 5) * G::PLANE_UNITS + (y & 31) * M + col, pol);
         } else {
           const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
           v[j1] = rem[(y & 31) * M + col];
@@ -214,6 +220,7 @@ template <int N, class T> struct Plane {
     if (tid < 16 * M1) {
       const int c = tid & 15, k1 = tid >> 4;
       const int col = rank * kCols + c;
+      const uint64_t spol = l2_stream_policy();
       T2 u[16];
 #pragma unroll
       for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
@@ -221,7 +228,7 @@ template <int N, class T> struct Plane {
 #pragma unroll
       for (int k2 = 0; k2 < 16; k2++) {
         const int ky = k1 + M1 * k2;
-        dst[((size_t)plane * N + ky) * M + col] = u[k2];
+        st_stream(dst + ((size_t)plane * N + ky) * M + col, u[k2], spol);
       }
     }
   }
@@ -256,7 +263,10 @@ template <int N, class T> struct Plane {
       for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
       Dft<+1, 16, T2>::run(u);
 #pragma unroll
-      for (int k2 = 0; k2 < 16; k2++) (XG ? gx : buf)[k1 * 256 + k2 * 16 + c] = u[k2];  // = ycol(k1 + M1*k2, c)
+      for (int k2 = 0; k2 < 16; k2++) {  // to ycol(k1 + M1*k2, c)
+        if constexpr (XG) st_keep(gx + k1 * 256 + k2 * 16 + c, u[k2], l2_keep_policy());
+        else buf[k1 * 256 + k2 * 16 + c] = u[k2];
+      }
     }
     cluster.sync();
   }
@@ -280,8 +290,9 @@ template <int N, class T> struct Plane {
     static_assert(N1 % 2 == 0, "pairs");
     const int j2 = tid & 7, r = tid >> 3, lane = tid & 31;
     const int y = rank * kRows + r;
+    const uint64_t pol = XG ? l2_keep_policy() : 0;
     auto col = [&](int q) -> T2 {  // X_q of row y from its column owner
-      if constexpr (XG) return __ldcg(gp + (size_t)(q / kCols) * G::PLANE_UNITS + ycol(y, q % kCols));
+      if constexpr (XG) return ld_keep(gp + (size_t)(q / kCols) * G::PLANE_UNITS + ycol(y, q % kCols), pol);
       else return cluster.map_shared_rank(buf, (unsigned)(q / kCols))[ycol(y, q % kCols)];
     };
     T2 v[N1], w[H];
@@ -416,6 +427,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
   const XgAreas<N, T> xa(p, rank);
+  const uint64_t spol = l2_stream_policy();  // streamed field data
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   const T *src = reinterpret_cast<const T *>(p.in[b]);
   T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
       sfor<0, N1>([&](auto J1) {
         constexpr int j1 = SPM_CI(J1);
         const int j = j1 * 8 + j2;
-        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : __ldg(row + j), acc);
+        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : ld_stream(row + j, spol), acc);
       });
       P::zf1_store(buf, ztw, v, r, j2);
     }
@@ -739,6 +751,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
   const XgAreas<N, T> xa(p, rank);
+  const uint64_t spol = l2_stream_policy();  // streamed field data
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   auto issue = [&](int plane) {  // thread 0: one tensor box (this CTA's 16 columns x all ky)
     mbar_expect_tx(bar, (unsigned)(N * 16 * sizeof(T2)));
@@ -768,7 +781,8 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     P::template yi<(XG & kXgInv) != 0>(
         buf, tw, tid, cluster,
         [&](int ky, int c) -> T2 {
-          return STAGED ? stage[ky * 16 + c] : __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c);
+          return STAGED ? stage[ky * 16 + c]
+                        : ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c, spol);
         },
         xa.own[it & 1]);  // alternating areas, as in plane_fwd
     if (STAGED && tid == 0 && next < N) {
@@ -825,6 +839,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
   const XgAreas<N, T> xa(p, rank);
+  const uint64_t spol = l2_stream_policy();  // streamed field data
   const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
   plane_twiddles<N, T>(p, tw, ztw);
   double acc_e[NE > 0 ? NE : 1], acc_p[NP > 0 ? NP : 1];
@@ -843,7 +858,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
       prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + tid) * M + rank * kCols, kCols * sizeof(T2));
     P::template yi<(XG & kXgInv) != 0>(
         buf, tw, tid, cluster,
-        [&](int ky, int c) -> T2 { return __ldg(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c); },
+        [&](int ky, int c) -> T2 { return ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c, spol); },
         xa.own[0]);
     P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[0]);
     if (stop) {
