@@ -416,11 +416,11 @@ def main():
         for knob, v in zip(("plane_cps", "fuse_planes", "plane_xg"), args.schedule.split(",")):
             ctx.tune(knob, int(v))
     else:
-        ctx.autotune(20)
+        ctx.autotune(60)
     sched64 = ctx.tuning()
     _c32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
     if not args.schedule:
-        _c32.autotune(20)
+        _c32.autotune(60)
     sched32 = _c32.tuning()
     _c32.close()
     phi_h = initial_field(1 + rank)
@@ -519,7 +519,7 @@ def main():
     # FP32 bulk (same workload, FP32 transforms, FP64 reductions)
     ctx32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
     if not args.schedule:
-        ctx32.autotune(20)  # the remembered FP32 choice
+        ctx32.autotune(60)  # the remembered FP32 choice
     phi32 = torch.from_numpy(phi_h.astype(np.float32)).cuda()
     uh32 = ctx32.my_fft(phi32)
     run_steps(args.warmup, phi32, uh32, ctx32)
