@@ -71,6 +71,10 @@ size_t footprint_of(const spm_job_desc &d) {
       break;
     default: fields = 4;
   }
+  // an FP32 twin may take the plane exchange areas of an earlier FP32
+  // autotune in this process: at most 2 x (N x N/32 CTAs) x 16 N FP32 complex
+  // values = one FP64 field
+  if (mixed) fields += 1;
   const double tables = (3.0 * (d.N / 2) * (d.N / 2) + 1) * 32 + d.N * 16.0;
   return (size_t)(fields * fb + tables) + (8u << 20);
 }
