@@ -134,7 +134,7 @@ def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
     assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
 
 
-@pytest.mark.parametrize("N,prec", [(64, "fp64"), (256, "fp64"), (128, "fp32")])
+@pytest.mark.parametrize("N,prec", [(64, "fp64"), (96, "fp64"), (256, "fp64"), (128, "fp32"), (192, "fp32")])
 def test_exchange_routes_are_bit_identical(spm, cuda, N, prec):
     """Gradient chains whose plane kernels exchange through global areas in L2
     (plane_xg 1, 2, 3; plane_cps 2 and 3) give the same fields as exchanges
