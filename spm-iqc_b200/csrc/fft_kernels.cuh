@@ -520,6 +520,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
   const int pen = tid & 15, rowsel = pen >> 3, cc = pen & 7;
+  const uint64_t spol = l2_stream_policy();  // outputs: evict first
   const bool has2 = (tid >> 4) < M1;  // owns a stage-2 task (pencil, k1)
   const int k1 = tid >> 4;
   // Tiles run columns-fastest, so concurrently resident CTAs read adjacent
@@ -679,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
         } else {
           Op::point(p, b, Kx, Ky, col, sym_at(Kx, Ky, col, cc), f, s, o_st, o_inv, acc, dc && cc == 0 ? 1.0 : 2.0);
         }
-        if constexpr (Op::SO) so[((size_t)kx * N + ky) * M + col] = o_st;
+        if constexpr (Op::SO) st_stream(so + ((size_t)kx * N + ky) * M + col, o_st, spol);
         F[k2] = o_inv;
       }
     }
@@ -707,7 +708,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
         sfor<0, M1>([&](auto J1) {
           constexpr int j1 = SPM_CI(J1);
           const int x = 16 * j1 + j2;
-          dst[((size_t)x * N + ky) * M + col] = v[j1];
+          st_stream(dst + ((size_t)x * N + ky) * M + col, v[j1], spol);
         });
       }
       __syncthreads();
