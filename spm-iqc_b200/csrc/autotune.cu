@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "../../include/spmiqc.h"
 #include "spm_internal.h"
@@ -87,7 +88,9 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   // plane variant, fused plane pass, exchange routes of the gradient chains
   const Choice cands[] = {{2, 1, 0}, {3, 1, 0}, {1, 1, 0}, {2, 0, 0}, {2, 1, spm::kXgFwd | spm::kXgInv},
                           {3, 1, spm::kXgFwd | spm::kXgInv}, {2, 1, spm::kXgFwd}, {2, 1, spm::kXgInv}};
-  for (const Choice &cand : cands) {
+  std::vector<Choice> all(std::begin(cands), std::end(cands));
+  if (c->prec == SPM_FP32) all.push_back({4, 1, spm::kXgFwd | spm::kXgInv});  // four CTAs per SM
+  for (const Choice &cand : all) {
     if (rc != SPM_OK) break;
     c->plane_cps = cand.plane_cps;
     c->fuse_planes = cand.fuse_planes;

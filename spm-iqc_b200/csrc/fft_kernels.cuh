@@ -815,7 +815,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
 // flow stops (the pencil pass armed FW_PENDING): the forward half is then
 // skipped. A chain of K steps is plane_fwd, K pencils, K-1 of these and one
 // plane_inv, so the real field crosses HBM once per chain instead of twice per
-// step. Direct loads; CPS (2 or 3) CTAs per SM, the layout of plane_fwd's
+// step. Direct loads; CPS (2, 3 or 4) CTAs per SM, the layout of plane_fwd's
 // direct variant.
 template <int N, class T, class Epi, class Pro, int CPS, int XG = 0>
 __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {

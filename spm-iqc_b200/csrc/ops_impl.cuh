@@ -77,13 +77,23 @@ template <class X> struct XgOk : std::false_type {};
 template <class T> struct XgOk<ProGrad<T>> : std::true_type {};
 template <class T> struct XgOk<EpiFlow<T>> : std::true_type {};
 static inline int xg_bits(const spm_ctx *c, int nb) { return (c->xg && nb == 1 && c->plane_cps >= 2) ? c->plane_xg : 0; }
+// Four CTAs per SM (64 registers per thread): FP32 gradient chains only.
+template <class T> static inline bool cps4(const spm_ctx *c) { return sizeof(T) == 4 && c->plane_cps == 4; }
 
-// The plane kernels come in three variants (c->plane_cps): 1 = staged, one
-// CTA per SM; 2 = direct loads, two CTAs per SM; 3 = direct, three CTAs per SM.
+// The plane kernels come in four variants (c->plane_cps): 1 = staged, one CTA
+// per SM; 2 = direct loads, two CTAs per SM; 3 = direct, three CTAs per SM;
+// 4 = direct, four CTAs per SM for FP32 gradient chains (3 elsewhere).
 template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
   if constexpr (XgOk<Pro>::value) {
     if (xg_bits(c, nb) & kXgFwd) {
-      if (c->plane_cps == 3) {
+      if constexpr (sizeof(T) == 4) {
+        if (cps4<T>(c)) {
+          struct Tag4x {};
+          return launch_cluster<Tag4x, N>(c, plane_fwd_kernel<N, T, Pro, 4, kXgFwd>, plane_smem<N, T, 4>(), p, nb,
+                                          "plane_fwd", true);
+        }
+      }
+      if (c->plane_cps >= 3) {
         struct Tag3x {};
         return launch_cluster<Tag3x, N>(c, plane_fwd_kernel<N, T, Pro, 3, kXgFwd>, plane_smem<N, T, 3>(), p, nb,
                                         "plane_fwd", true);
@@ -93,7 +103,7 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
                                       "plane_fwd", true);
     }
   }
-  if (c->plane_cps == 3) {
+  if (c->plane_cps >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_fwd_kernel<N, T, Pro, 3>, plane_smem<N, T, 3>(), p, nb, "plane_fwd");
   }
@@ -107,7 +117,14 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
 template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p0, int nb) {
   if constexpr (XgOk<Epi>::value) {
     if (xg_bits(c, nb) & kXgInv) {
-      if (c->plane_cps == 3) {
+      if constexpr (sizeof(T) == 4) {
+        if (cps4<T>(c)) {
+          struct Tag4x {};
+          return launch_cluster<Tag4x, N>(c, plane_inv_kernel<N, T, Epi, 4, kXgInv>, plane_smem<N, T, 4>(), p0, nb,
+                                          "plane_inv", true);
+        }
+      }
+      if (c->plane_cps >= 3) {
         struct Tag3x {};
         return launch_cluster<Tag3x, N>(c, plane_inv_kernel<N, T, Epi, 3, kXgInv>, plane_smem<N, T, 3>(), p0, nb,
                                         "plane_inv", true);
@@ -117,7 +134,7 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
                                       "plane_inv", true);
     }
   }
-  if (c->plane_cps == 3) {
+  if (c->plane_cps >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_inv_kernel<N, T, Epi, 3>, plane_smem<N, T, 3>(), p0, nb, "plane_inv");
   }
@@ -134,7 +151,14 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
 // three with plane_cps = 3), with the exchange routes XG.
 template <int N, class T, class Epi, class Pro, int XG>
 static int plane_inv_fwd_xg(spm_ctx *c, const KParams &p, int nb) {
-  if (c->plane_cps == 3) {
+  if constexpr (sizeof(T) == 4 && XG != 0) {
+    if (cps4<T>(c)) {
+      struct Tag4 {};
+      return launch_cluster<Tag4, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 4, XG>, plane_smem<N, T, 4>(), p, nb,
+                                     "plane_inv_fwd", true);
+    }
+  }
+  if (c->plane_cps >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 3, XG>, plane_smem<N, T, 3>(), p, nb,
                                    "plane_inv_fwd", XG != 0);
