@@ -579,6 +579,17 @@ def main():
         spmiqc.check(L_.spm_grad_flow_host(ctx.h, ph_host.data_ptr(), 1, 0.0, rec, ctypes.byref(nd)))
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = world * e2e_steps / e2e_s
+    # the same through one call per K steps (the reference's get_min_u_F runs
+    # its whole loop per call): upload phi, K steps, download phi and the K
+    # step records
+    K = args.steps
+    recs = (spmiqc.StepStats * K)()
+    barrier(world)
+    t0 = time.perf_counter()
+    spmiqc.check(L_.spm_grad_flow_host(ctx.h, ph_host.data_ptr(), K, 0.0, recs, ctypes.byref(nd)))
+    call_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_call = {"value": world * nd.value / call_s, "unit": "steps/s", "steps_per_call": nd.value,
+                "h2d_bytes_per_step": S / K, "d2h_bytes_per_step": (S + 32 * K) / K}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -610,6 +621,7 @@ def main():
             "clocks": clk,
             "gpu_launches": int(launches),
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": S, "d2h_bytes_per_step": S + 32},
+            "e2e_per_call": e2e_call,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
