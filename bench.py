@@ -516,6 +516,37 @@ def main():
     hv_per_s = 8 * reps / (h0.elapsed_time(h1) / 1000.0)
     del V, HV
 
+    # LOBPCG (k = 8, the reference's 21 iterations per call) and SPM spring-pair
+    # iterations on the same field, one call each after a warm-up call
+    solvers = {}
+    try:
+        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
+        ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=2)
+        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev, rs, its = ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=21)
+        torch.cuda.synchronize()
+        dt_l = time.perf_counter() - t0
+        solvers["lobpcg_k8"] = {"seconds_per_call": dt_l, "iterations": its, "iterations_per_s": its / dt_l,
+                                "max_residual": float(max(rs))}
+        v1 = Vb[0].clone()
+        del Vb
+        p0 = phi.clone()
+        p1 = phi + 0.001 * v1
+        ctx.Spring_Pairing(p0, p1, 2, 0.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hist = ctx.Spring_Pairing(p0, p1, 50, 0.0)
+        torch.cuda.synchronize()
+        dt_s = time.perf_counter() - t0
+        solvers["spm"] = {"iterations": len(hist), "iterations_per_s": len(hist) / dt_s,
+                          "last_residual": float(hist[-1])}
+        del p0, p1, v1
+    except Exception as ex:  # a solver leg that fails is reported, not fatal
+        solvers["error"] = str(ex)[:200]
+    torch.cuda.empty_cache()
+
     # FP32 bulk (same workload, FP32 transforms, FP64 reductions)
     ctx32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
     if not args.schedule:
@@ -611,7 +642,7 @@ def main():
                        "l2": "inputs larger than L2 (0.81 GB of fields through HBM per step)",
                        "schedule_fp64": sched64, "schedule_fp32": sched32},
             "p50_ms": p50, "p99_ms": p99,
-            "hv_per_s": hv_per_s, "fp32_steps_per_s": fp32_value, "precision": precision,
+            "hv_per_s": hv_per_s, "solvers_256_fp64": solvers, "fp32_steps_per_s": fp32_value, "precision": precision,
             "kernels_ms": dict(zip(names, kms)),
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,

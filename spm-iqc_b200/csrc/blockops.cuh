@@ -15,7 +15,7 @@ struct GramP {
   const void *X[kBlkMax];
   const void *Y[kBlkMax];
   int ma, mb;
-  size_t n;          // points per vector (multiple of 4)
+  size_t n;          // points per vector (multiple of 8)
   double inv_n;      // normalisation of <.,.> (1/N^3)
   double *partials;  // [kGramBlocks][kBlkMax * kBlkMax]
   unsigned *ticket;
@@ -31,50 +31,65 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 
 // G[a][b] = inv_n * sum_i X_a[i] Y_b[i] for a < ma, b < mb (the Gram of
 // LOBPCG.cpp:343-358 and the inner products of the block orthogonalisations).
-// Each warp owns interleaved 4-point k-steps and accumulates the (ma x mb)
-// product in 8x8 FP64 MMA tiles; CTA and grid totals are summed in a fixed
-// order, so the result does not depend on scheduling.
-template <class T>
+// Each warp owns interleaved 8-point k-steps, two at a time: lane (row, tig)
+// loads points 2 tig and 2 tig + 1 of the step with one vector load and feeds
+// them to two MMAs (the same point order for X and Y, so the k order is
+// merely permuted), accumulating the (ma x mb) product in 8x8 FP64 MMA tiles;
+// CTA and grid totals are summed in a fixed order, so the result does not
+// depend on scheduling.
+// U = k-steps loaded per loop iteration, TM = row tiles (8 vectors each) at
+// most per operand: (4, 1), (4, 2) or (2, 3) by block size.
+template <class T, int U, int TM>
 __global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_constant__ GramP p) {
   __shared__ int s_last;
   if (p.flow && *((volatile const int *)p.flow) == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const int TA = (p.ma + 7) >> 3, TB = (p.mb + 7) >> 3;
-  double acc[3][3][2];
+  double acc[TM][TM][2];
 #pragma unroll
-  for (int i = 0; i < 3; i++)
+  for (int i = 0; i < TM; i++)
 #pragma unroll
-    for (int j = 0; j < 3; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-  const T *xr[3], *yr[3];
+    for (int j = 0; j < TM; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  using V2 = c2<T>;
+  const V2 *xr[TM], *yr[TM];
 #pragma unroll
-  for (int t = 0; t < 3; t++) {
+  for (int t = 0; t < TM; t++) {
     const int ra = t * 8 + gid, rb = t * 8 + gid;
-    xr[t] = (t < TA && ra < p.ma) ? reinterpret_cast<const T *>(p.X[ra]) : nullptr;
-    yr[t] = (t < TB && rb < p.mb) ? reinterpret_cast<const T *>(p.Y[rb]) : nullptr;
+    xr[t] = (t < TA && ra < p.ma) ? reinterpret_cast<const V2 *>(p.X[ra]) : nullptr;
+    yr[t] = (t < TB && rb < p.mb) ? reinterpret_cast<const V2 *>(p.Y[rb]) : nullptr;
   }
-  const size_t steps = p.n / 4;
+  const size_t steps = p.n / 8;
   const size_t gw = (size_t)blockIdx.x * kGramWarps + warp, W = (size_t)gridDim.x * kGramWarps;
-  for (size_t s = gw; s < steps; s += W) {
-    const size_t k = 4 * s + tig;
-    double a[3], b[3];
+  for (size_t s = gw; s < steps; s += U * W) {
+    V2 a[U][TM], b[U][TM];
 #pragma unroll
-    for (int t = 0; t < 3; t++) {
-      a[t] = xr[t] ? (double)__ldg(xr[t] + k) : 0.0;
-      b[t] = yr[t] ? (double)__ldg(yr[t] + k) : 0.0;
+    for (int u = 0; u < U; u++) {
+      const size_t su = s + u * W;
+      const bool in = su < steps;
+#pragma unroll
+      for (int t = 0; t < TM; t++) {
+        a[u][t] = (xr[t] && in) ? __ldg(xr[t] + 4 * su + tig) : V2{0, 0};
+        b[u][t] = (yr[t] && in) ? __ldg(yr[t] + 4 * su + tig) : V2{0, 0};
+      }
     }
 #pragma unroll
-    for (int i = 0; i < 3; i++)
+    for (int u = 0; u < U; u++)
 #pragma unroll
-      for (int j = 0; j < 3; j++)
-        if (i < TA && j < TB) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TM; j++)
+          if (i < TA && j < TB) {
+            dmma_8x8x4(acc[i][j][0], acc[i][j][1], (double)a[u][i].x, (double)b[u][j].x);
+            dmma_8x8x4(acc[i][j][0], acc[i][j][1], (double)a[u][i].y, (double)b[u][j].y);
+          }
   }
   // CTA total in a fixed warp order: warp w writes its tiles, warp 0 sums
   __shared__ double tile[kGramWarps][kBlkMax * kBlkMax];
 #pragma unroll
-  for (int i = 0; i < 3; i++)
+  for (int i = 0; i < TM; i++)
 #pragma unroll
-    for (int j = 0; j < 3; j++)
+    for (int j = 0; j < TM; j++)
       if (i < TA && j < TB) {
         const int r = i * 8 + gid, c = j * 8 + 2 * tig;
         tile[warp][r * kBlkMax + c] = acc[i][j][0];
@@ -117,8 +132,30 @@ struct CombP {
 };
 
 // Y_q[i] = (accumulate ? Y_q[i] : 0) + sum_p C[p][q] X_p[i] + d[q]. A point's
-// inputs are all read before its outputs are written, so Y may alias X.
-template <class T>
+// inputs (and, accumulating, its old outputs) are all loaded before any of its
+// outputs is written, so Y may alias X and every load of a point is in flight
+// at once. MI / MO bound nin / nout (registers); PTS consecutive points per
+// thread, loaded as one vector when 2.
+template <class T, int PTS> struct Pts;
+template <class T> struct Pts<T, 1> {
+  static __device__ __forceinline__ void ld(const void *b, size_t i, double (&v)[1]) {
+    v[0] = (double)reinterpret_cast<const T *>(b)[i];
+  }
+  static __device__ __forceinline__ void st(void *b, size_t i, const double (&v)[1]) {
+    reinterpret_cast<T *>(b)[i] = (T)v[0];
+  }
+};
+template <class T> struct Pts<T, 2> {
+  static __device__ __forceinline__ void ld(const void *b, size_t i, double (&v)[2]) {
+    const c2<T> w = reinterpret_cast<const c2<T> *>(b)[i];
+    v[0] = (double)w.x;
+    v[1] = (double)w.y;
+  }
+  static __device__ __forceinline__ void st(void *b, size_t i, const double (&v)[2]) {
+    reinterpret_cast<c2<T> *>(b)[i] = c2<T>{(T)v[0], (T)v[1]};
+  }
+};
+template <class T, int MI, int MO, int PTS>
 __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ CombP p) {
   __shared__ double sc[(kBlkMax + 8) * kBlkMax + kBlkMax];
   if (p.flow && *((volatile const int *)p.flow) == 0) return;
@@ -126,18 +163,37 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
   for (int e = threadIdx.x; e < p.nout; e += blockDim.x) sc[(kBlkMax + 8) * kBlkMax + e] = p.d ? p.d[e] : 0.0;
   __syncthreads();
   const double *dd = sc + (kBlkMax + 8) * kBlkMax;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (size_t)gridDim.x * blockDim.x) {
-    double x[kBlkMax + 8];
+  const size_t nv = p.n / PTS;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (size_t)gridDim.x * blockDim.x) {
+    double x[MI][PTS], y[MO][PTS];
 #pragma unroll
-    for (int q = 0; q < kBlkMax + 8; q++) x[q] = (q < p.nin) ? (double)reinterpret_cast<const T *>(p.X[q])[i] : 0.0;
-#pragma unroll 1
-    for (int q = 0; q < p.nout; q++) {
-      T *yq = reinterpret_cast<T *>(p.Y[q]);
-      double s = p.accumulate ? (double)yq[i] : 0.0;
+    for (int q = 0; q < MI; q++) {
+      if (q < p.nin) Pts<T, PTS>::ld(p.X[q], i, x[q]);
+      else
 #pragma unroll
-      for (int r = 0; r < kBlkMax + 8; r++)
-        if (r < p.nin) s += sc[r * p.nout + q] * x[r];
-      yq[i] = (T)(s + dd[q]);
+        for (int e = 0; e < PTS; e++) x[q][e] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < MO; q++) {
+      if (q < p.nout && p.accumulate) Pts<T, PTS>::ld(p.Y[q], i, y[q]);
+      else
+#pragma unroll
+        for (int e = 0; e < PTS; e++) y[q][e] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < MO; q++) {
+      if (q < p.nout) {
+        double o[PTS];
+#pragma unroll
+        for (int e = 0; e < PTS; e++) {
+          double s = y[q][e];
+#pragma unroll
+          for (int r = 0; r < MI; r++)
+            if (r < p.nin) s += sc[r * p.nout + q] * x[r][e];
+          o[e] = s + dd[q];
+        }
+        Pts<T, PTS>::st(p.Y[q], i, o);
+      }
     }
   }
 }

@@ -79,8 +79,15 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
   p.ticket = s->gram_ticket;
   p.out = s->gram_out;
   c->launches++;
-  if (c->prec == SPM_FP64) gram_kernel<double><<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
-  else gram_kernel<float><<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
+  // blocks of up to 8 / 16 vectors: four k-steps per loop iteration; up to 24: two
+  const int tiles = (std::max(ma, mb) + 7) / 8;
+  auto launch = [&](auto kd, auto kf) {
+    if (c->prec == SPM_FP64) kd<<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
+    else kf<<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
+  };
+  if (tiles == 1) launch(gram_kernel<double, 4, 1>, gram_kernel<float, 4, 1>);
+  else if (tiles == 2) launch(gram_kernel<double, 4, 2>, gram_kernel<float, 4, 2>);
+  else launch(gram_kernel<double, 2, 3>, gram_kernel<float, 2, 3>);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->h_gram, s->gram_out, sizeof(double) * ma * mb, cudaMemcpyDeviceToHost, c->stream);
@@ -115,8 +122,15 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
   p.d = d ? s->coef + (size_t)nin * nout : nullptr;
   p.accumulate = acc ? 1 : 0;
   c->launches++;
-  if (c->prec == SPM_FP64) combine_kernel<double><<<1184, 256, 0, c->stream>>>(p);
-  else combine_kernel<float><<<1184, 256, 0, c->stream>>>(p);
+  // register-bounded variants by block shape (two points per thread where they fit)
+  auto launch = [&](auto kd, auto kf) {
+    if (c->prec == SPM_FP64) kd<<<1184, 256, 0, c->stream>>>(p);
+    else kf<<<1184, 256, 0, c->stream>>>(p);
+  };
+  if (nin <= 8 && nout <= 8) launch(combine_kernel<double, 8, 8, 2>, combine_kernel<float, 8, 8, 2>);
+  else if (nin <= 16 && nout <= 8) launch(combine_kernel<double, 16, 8, 1>, combine_kernel<float, 16, 8, 1>);
+  else if (nout <= 8) launch(combine_kernel<double, kBlkMax + 8, 8, 1>, combine_kernel<float, kBlkMax + 8, 8, 1>);
+  else launch(combine_kernel<double, kBlkMax + 8, kBlkMax, 1>, combine_kernel<float, kBlkMax + 8, kBlkMax, 1>);
   e = cudaGetLastError();
   return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "combine launch");
 }
