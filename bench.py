@@ -369,6 +369,65 @@ def serve_bench(args):
     return 0
 
 
+def solver_legs(ctx, phi):
+    """LOBPCG (k = 8, the reference's 21 iterations per call) and 50 SPM
+    spring-pair iterations (replicas phi and phi + 0.001 v1) on the field phi,
+    one timed call each after a warm-up call."""
+    import torch
+    solvers = {}
+    try:
+        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
+        ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=2)
+        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev, rs, its = ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=21)
+        torch.cuda.synchronize()
+        dt_l = time.perf_counter() - t0
+        solvers["lobpcg_k8"] = {"seconds_per_call": dt_l, "iterations": its, "iterations_per_s": its / dt_l,
+                                "max_residual": float(max(rs))}
+        v1 = Vb[0].clone()
+        del Vb
+        p0 = phi.clone()
+        p1 = phi + 0.001 * v1
+        ctx.Spring_Pairing(p0, p1, 2, 0.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hist = ctx.Spring_Pairing(p0, p1, 50, 0.0)
+        torch.cuda.synchronize()
+        dt_s = time.perf_counter() - t0
+        solvers["spm"] = {"iterations": len(hist), "iterations_per_s": len(hist) / dt_s,
+                          "last_residual": float(hist[-1])}
+        del p0, p1, v1
+    except Exception as ex:  # a solver leg that fails is reported, not fatal
+        solvers["error"] = str(ex)[:200]
+    torch.cuda.empty_cache()
+    return solvers
+
+
+def solvers_bench(args):
+    """LOBPCG and SPM iterations at 256^3 FP64 on the bench field after 100
+    gradient steps (one JSON line; also the command of their ncu captures)."""
+    import torch
+    import spmiqc
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp64")
+    phi = torch.from_numpy(initial_field(1 + rank)).cuda()
+    uh = ctx.my_fft(phi)
+    ctx.get_min_u_F(phi, uh, 100)
+    out = solver_legs(ctx, phi)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": "LOBPCG k=8 iterations/s and SPM iterations/s (256^3 FP64)",
+                          "solvers_256_fp64": out, "n_gpus": world, "data": "synthetic",
+                          "config": {"workload": "bench field after 100 gradient steps", "N": N}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,6 +446,7 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--batch", action="store_true", help="run the batched-relaxation workload instead (one JSON line)")
     ap.add_argument("--batch-n", type=int, default=24)
+    ap.add_argument("--solvers", action="store_true", help="run only the LOBPCG and SPM legs (one JSON line)")
     ap.add_argument("--batch-steps", type=int, default=4000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -394,6 +454,8 @@ def main():
         return serve_bench(args)
     if args.batch:
         return batch_bench(args)
+    if args.solvers:
+        return solvers_bench(args)
     rank, world, local = dist_setup()
     if args.impl == "reference":
         rc = reference_arm(args, rank, world)
@@ -516,36 +578,7 @@ def main():
     hv_per_s = 8 * reps / (h0.elapsed_time(h1) / 1000.0)
     del V, HV
 
-    # LOBPCG (k = 8, the reference's 21 iterations per call) and SPM spring-pair
-    # iterations on the same field, one call each after a warm-up call
-    solvers = {}
-    try:
-        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
-        ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=2)
-        Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ev, rs, its = ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=21)
-        torch.cuda.synchronize()
-        dt_l = time.perf_counter() - t0
-        solvers["lobpcg_k8"] = {"seconds_per_call": dt_l, "iterations": its, "iterations_per_s": its / dt_l,
-                                "max_residual": float(max(rs))}
-        v1 = Vb[0].clone()
-        del Vb
-        p0 = phi.clone()
-        p1 = phi + 0.001 * v1
-        ctx.Spring_Pairing(p0, p1, 2, 0.0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        hist = ctx.Spring_Pairing(p0, p1, 50, 0.0)
-        torch.cuda.synchronize()
-        dt_s = time.perf_counter() - t0
-        solvers["spm"] = {"iterations": len(hist), "iterations_per_s": len(hist) / dt_s,
-                          "last_residual": float(hist[-1])}
-        del p0, p1, v1
-    except Exception as ex:  # a solver leg that fails is reported, not fatal
-        solvers["error"] = str(ex)[:200]
-    torch.cuda.empty_cache()
+    solvers = solver_legs(ctx, phi)
 
     # FP32 bulk (same workload, FP32 transforms, FP64 reductions)
     ctx32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
