@@ -48,7 +48,7 @@ struct spm_ctx {
   int *gate = nullptr;          // flow words gating every launch of a solver chain (or null)
   double *gtab = nullptr;       // spectral symbols per K^2 (4 doubles each)
   std::vector<TmEntry> tmaps;   // tensor-map cache (most recent last)
-  int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged, 2 direct)
+  int plane_cps = 2;            // plane-kernel variant: CTAs per SM (1 staged; 2, 3 direct; 4 FP32 chains)
   int fuse_planes = 1;          // gradient chains use the fused inverse -> forward plane pass
   int plane_xg = 0;             // gradient-chain plane kernels: exchanges through L2 (spm::kXgFwd | kXgInv bits)
   void *xg = nullptr;           // their global exchange areas (2 x xg_cap CTAs x 16 N complex)
