@@ -60,3 +60,23 @@ def test_dropin_matches_reference(cuda):
     assert rel(q2, q1) < 1e-9
     ref.close()
     gpu.close()
+
+
+def test_long_spring_pairing_matches_reference(cuda):
+    """120 spring-pair iterations through the C ABI against the reference's own
+    Spring_Pairing (compiled here) on the same replicas: the two runs stay
+    together over a long trajectory, not only over the first steps."""
+    import spmiqc
+    N = 32
+    ref = refbind.Ref(N, Tau=-0.01)
+    phi = npo.uniform_field(N, 21)
+    d = npo.uniform_field(N, 22, amp=1.0)
+    a, b = phi, phi + 0.001 * d / np.sqrt(np.mean(d * d))
+    for _ in range(3):  # the reference restarts its loop per call, as the C ABI does
+        a, b = ref.spring_pairing(a, b, 40, 1e-14)
+    ctx = spmiqc.SpmContext(N, Tau=-0.01)
+    p0 = cuda.from_numpy(phi.copy()).cuda()
+    p1 = cuda.from_numpy(phi + 0.001 * d / np.sqrt(np.mean(d * d))).cuda()
+    for _ in range(3):
+        ctx.Spring_Pairing(p0, p1, 40, 1e-14)
+    assert rel(p0.cpu().numpy(), a) < 1e-9 and rel(p1.cpu().numpy(), b) < 1e-9
