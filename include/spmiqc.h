@@ -85,7 +85,8 @@ const char *spm_status_str(int status);
  * input in shared memory (one CTA per SM), 2 = direct loads, two CTAs per SM,
  * 3 = direct loads, three CTAs per SM (fewer registers per thread), 4 = four
  * CTAs per SM for the exchanges through L2 of FP32 gradient chains (3
- * elsewhere).
+ * elsewhere), 5 = CTAs of 16 rows and 128 threads, four per SM, for gradient
+ * chains with both exchanges through L2 (2 elsewhere).
  * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
  * inverse plane pass with the next step's forward one (phi stays on chip
  * between steps; the same bits as 0), 0 = three passes per step.
@@ -101,7 +102,7 @@ int spm_tune_get(const spm_ctx *ctx, const char *knob);
 /* Autotuner (no counterpart in the reference): times chains of `steps`
  * gradient steps on a scratch field for each candidate schedule (plane_cps
  * 1/2/3 with fused chains, plane_cps 2 without, plane_xg 1/2/3 with plane_cps
- * 2 and 3 on fused chains, plane_cps 4 for FP32) and keeps the fastest in the
+ * 2 and 3 on fused chains, plane_cps 4 for FP32, 5) and keeps the fastest in the
  * context; the choice is remembered per (device, N, precision), so later
  * contexts of the same kind take it without timing (FP32 twins of mixed flows
  * included). Synchronises; allocates two scratch fields while it runs. The

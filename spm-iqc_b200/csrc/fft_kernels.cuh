@@ -40,8 +40,8 @@ template <int N> struct Geo {
 
 // Shared-memory layout (complex units): twiddles N | z-twiddles N/2 | work | stage | mbarriers | reduction
 // (+128 bytes to align the base for the tensor copies)
-template <int N, class T, int CPS> constexpr size_t plane_smem() {
-  return sizeof(c2<T>) * (N + N / 2 + Geo<N>::PLANE_UNITS + (CPS == 1 ? Geo<N>::STAGE_UNITS : 0)) + 16 +
+template <int N, class T, int CPS, int RW = kRows> constexpr size_t plane_smem() {
+  return sizeof(c2<T>) * (N + N / 2 + RW * (N / 2) + (CPS == 1 ? Geo<N>::STAGE_UNITS : 0)) + 16 +
          sizeof(double) * 32 * kRedMax + 128;
 }
 // Pencil symbol table (per tile): 9 kz rows (the tile's 8 columns and kz = N/2)
@@ -62,16 +62,19 @@ __device__ __forceinline__ bool flow_stopped(const KParams &p) {
 
 // This CTA's global exchange area (e = 0: inverse exchange, 1: forward) and
 // that of rank 0 of its cluster (the cluster's CTAs are consecutive in x).
-template <int N, class T> struct XgAreas {
+// Each of the two regions holds xg_cap areas of 16 N complex values (32-row
+// CTAs), or twice as many of 8 N (16-row CTAs).
+template <int N, class T, int RW = kRows> struct XgAreas {
   c2<T> *own[2] = {nullptr, nullptr};
   const c2<T> *first[2] = {nullptr, nullptr};
   __device__ XgAreas(const KParams &p, int rank) {
     if (p.xg == nullptr) return;
-    constexpr size_t U = Geo<N>::PLANE_UNITS;
+    constexpr size_t U = (size_t)RW * (N / 2);
+    const size_t region = (size_t)p.xg_cap * Geo<N>::PLANE_UNITS;
     c2<T> *xg = reinterpret_cast<c2<T> *>(p.xg);
     for (int e = 0; e < 2; e++) {
-      own[e] = xg + ((size_t)e * p.xg_cap + blockIdx.x) * U;
-      first[e] = xg + ((size_t)e * p.xg_cap + blockIdx.x - rank) * U;
+      own[e] = xg + e * region + (size_t)blockIdx.x * U;
+      first[e] = xg + e * region + (size_t)(blockIdx.x - rank) * U;
     }
   }
 };
@@ -82,18 +85,24 @@ __device__ __forceinline__ void report_error(const KParams &p, int s_err) {
 
 // --------------------------------------------------------------- plane phases
 // The line-transform phases of the plane passes, shared by plane_fwd,
-// plane_inv and the fused plane_inv_fwd. A CTA of a cluster owns kRows = 32
-// z-rows (real space) and kCols = 16 packed spectral columns of the current
-// x-plane; `buf` is its exchange area, which the other CTAs of the cluster
-// read through distributed shared memory.
-template <int N, class T> struct Plane {
+// plane_inv and the fused plane_inv_fwd. A CTA of a cluster owns RW z-rows
+// (real space; 32, or 16 in the variant with four CTAs per SM) and CW = RW/2
+// packed spectral columns of the current x-plane, with 8 RW threads; `buf` is
+// its exchange area, which the other CTAs of the cluster read through
+// distributed shared memory (or global areas, XG).
+template <int N, class T, int RW = kRows> struct Plane {
   using G = Geo<N>;
   using T2 = c2<T>;
   static constexpr int M = G::M, N1 = G::N1, M1 = G::M1;
+  static constexpr int CW = RW / 2;     // spectral columns per CTA
+  static constexpr int TH = 8 * RW;     // threads per CTA
+  static constexpr int CL = N / RW;     // CTAs per cluster = per x-plane
+  static constexpr int UNITS = RW * M;  // exchange units per CTA (= CW columns x N)
+  static constexpr int XS = 16 * CW;    // y-stage exchange stride per stage-1 output index
   // The z phases of a row stay inside one warp: warp w owns rows
   // RPW*w .. RPW*w + RPW - 1 in every z phase, and the z exchange of row r
   // lies inside row r's own M units, so those phases need only warp barriers.
-  static constexpr int RPW = kRows / (kThreads / 32);
+  static constexpr int RPW = RW / (TH / 32);
   static_assert(RPW * 8 == 32, "8 threads per row in the row-parallel z stages");
 
   // z-exchange slot of stage-1 output (j2, k1) of row r, rotated by j2 so the
@@ -181,25 +190,25 @@ template <int N, class T> struct Plane {
   // column c from the CTA holding row y, radix-M1 DFT, exchange, radix-16
   // DFT, store the spectral column into dst[plane][ky][M]. With XG the rows
   // come from the global exchange areas of the cluster's CTAs (gp = the area
-  // of rank 0; rank k's at gp + k * PLANE_UNITS), which stay untouched until
+  // of rank 0; rank k's at gp + k * UNITS), which stay untouched until
   // every CTA has passed the next plane's first cluster barrier, so no
   // "done reading" barrier is needed.
   template <bool XG = false>
   __device__ static void yf(T2 *buf, const T2 *tw, int tid, int rank, cg::cluster_group &cluster, T2 *dst,
                             int plane, const T2 *gp = nullptr) {
     {
-      const int c = tid & 15, j2 = tid >> 4;
-      const int col = rank * kCols + c;
+      const int c = tid % CW, j2 = tid / CW;
+      const int col = rank * CW + c;
       const uint64_t pol = XG ? l2_keep_policy() : 0;
       T2 v[M1];
       sfor<0, M1>([&](auto J1) {
         constexpr int j1 = SPM_CI(J1);
         const int y = 16 * j1 + j2;
         if constexpr (XG) {
-          v[j1] = ld_keep(gp + (size_t)(y >> 5) * G::PLANE_UNITS + (y & 31) * M + col, pol);
+          v[j1] = ld_keep(gp + (size_t)(y / RW) * UNITS + (y % RW) * M + col, pol);
         } else {
-          const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y >> 5));
-          v[j1] = rem[(y & 31) * M + col];
+          const T2 *rem = cluster.map_shared_rank(buf, (unsigned)(y / RW));
+          v[j1] = rem[(y % RW) * M + col];
         }
       });
       Dft<-1, M1, T2>::run(v);  // consumes every gathered value
@@ -213,17 +222,17 @@ template <int N, class T> struct Plane {
       if constexpr (!XG) cluster_wait();
       sfor<0, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
-        buf[k1 * 256 + j2 * 16 + c] = v[k1];
+        buf[k1 * XS + j2 * CW + c] = v[k1];
       });
     }
     __syncthreads();
-    if (tid < 16 * M1) {
-      const int c = tid & 15, k1 = tid >> 4;
-      const int col = rank * kCols + c;
+    if (tid < CW * M1) {
+      const int c = tid % CW, k1 = tid / CW;
+      const int col = rank * CW + c;
       const uint64_t spol = l2_stream_policy();
       T2 u[16];
 #pragma unroll
-      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * XS + j2 * CW + c];
       Dft<-1, 16, T2>::run(u);
 #pragma unroll
       for (int k2 = 0; k2 < 16; k2++) {
@@ -235,7 +244,7 @@ template <int N, class T> struct Plane {
 
   // Position of (y, column c) in the inverse-y output: stage 2 of task
   // (c, k1) writes its outputs y = k1 + M1*k2 back to the slots it read.
-  __device__ static int ycol(int y, int c) { return (y % M1) * 256 + (y / M1) * 16 + c; }
+  __device__ static int ycol(int y, int c) { return (y % M1) * XS + (y / M1) * CW + c; }
 
   // inverse y over this CTA's 16 columns; ld(ky, c) returns the input value.
   // Leaves y-line values at ycol(y, c) in buf (or, XG, in the CTA's global
@@ -243,7 +252,7 @@ template <int N, class T> struct Plane {
   template <bool XG = false, class LD>
   __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld, T2 *gx = nullptr) {
     {
-      const int c = tid & 15, j2 = tid >> 4;
+      const int c = tid % CW, j2 = tid / CW;
       T2 v[M1];
       sfor<0, M1>([&](auto J1) {
         constexpr int j1 = SPM_CI(J1);
@@ -252,20 +261,20 @@ template <int N, class T> struct Plane {
       Dft<+1, M1, T2>::run(v);
       sfor<0, M1>([&](auto K1) {
         constexpr int k1 = SPM_CI(K1);
-        buf[k1 * 256 + j2 * 16 + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
+        buf[k1 * XS + j2 * CW + c] = (k1 == 0) ? v[k1] : cmulc(v[k1], tw[j2 * k1]);
       });
     }
     __syncthreads();
-    if (tid < 16 * M1) {
+    if (tid < CW * M1) {
       T2 u[16];
-      const int c = tid & 15, k1 = tid >> 4;
+      const int c = tid % CW, k1 = tid / CW;
 #pragma unroll
-      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * 256 + j2 * 16 + c];
+      for (int j2 = 0; j2 < 16; j2++) u[j2] = buf[k1 * XS + j2 * CW + c];
       Dft<+1, 16, T2>::run(u);
 #pragma unroll
       for (int k2 = 0; k2 < 16; k2++) {  // to ycol(k1 + M1*k2, c)
-        if constexpr (XG) st_keep(gx + k1 * 256 + k2 * 16 + c, u[k2], l2_keep_policy());
-        else buf[k1 * 256 + k2 * 16 + c] = u[k2];
+        if constexpr (XG) st_keep(gx + k1 * XS + k2 * CW + c, u[k2], l2_keep_policy());
+        else buf[k1 * XS + k2 * CW + c] = u[k2];
       }
     }
     cluster.sync();
@@ -289,11 +298,11 @@ template <int N, class T> struct Plane {
     constexpr int H = N1 / 2;
     static_assert(N1 % 2 == 0, "pairs");
     const int j2 = tid & 7, r = tid >> 3, lane = tid & 31;
-    const int y = rank * kRows + r;
+    const int y = rank * RW + r;
     const uint64_t pol = XG ? l2_keep_policy() : 0;
     auto col = [&](int q) -> T2 {  // X_q of row y from its column owner
-      if constexpr (XG) return ld_keep(gp + (size_t)(q / kCols) * G::PLANE_UNITS + ycol(y, q % kCols), pol);
-      else return cluster.map_shared_rank(buf, (unsigned)(q / kCols))[ycol(y, q % kCols)];
+      if constexpr (XG) return ld_keep(gp + (size_t)(q / CW) * UNITS + ycol(y, q % CW), pol);
+      else return cluster.map_shared_rank(buf, (unsigned)(q / CW))[ycol(y, q % CW)];
     };
     T2 v[N1], w[H];
 #pragma unroll
@@ -392,9 +401,9 @@ template <int N, class T> struct Plane {
 // Loads the twiddles into shared memory: tw[j] = exp(-2 pi i j/N) and the
 // z-stage table ztw[k1*8 + j2] = w^{2 j2 k1}.
 template <int N, class T> __device__ __forceinline__ void plane_twiddles(const KParams &p, c2<T> *tw, c2<T> *ztw) {
-  for (int i = threadIdx.x; i < N; i += kThreads) tw[i] = reinterpret_cast<const c2<T> *>(p.tw)[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = reinterpret_cast<const c2<T> *>(p.tw)[i];
   __syncthreads();
-  for (int i = threadIdx.x; i < N / 2; i += kThreads) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
+  for (int i = threadIdx.x; i < N / 2; i += blockDim.x) ztw[i] = tw[(2 * (i & 7) * (i >> 3)) % N];
 }
 
 // --------------------------------------------------------------- plane_fwd
@@ -405,18 +414,19 @@ template <int N, class T> __device__ __forceinline__ void plane_twiddles(const K
 // CPS = CTAs per SM the variant is built for: 1 stages the next plane's rows
 // in shared memory with a bulk copy; 2 has no stage (half the shared memory,
 // so two CTAs share an SM) and loads its rows straight from global memory.
-template <int N, class T, class Pro, int CPS, int XG = 0>
-__global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
+template <int N, class T, class Pro, int CPS, int XG = 0, int RW = kRows>
+__global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
-  using P = Plane<N, T>;
+  using P = Plane<N, T, RW>;
   constexpr int N1 = G::N1;
   constexpr bool STAGED = (CPS == 1);
+  static_assert(!STAGED || RW == kRows, "the staged variant has 32-row CTAs");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
   T2 *ztw = tw + N;                  // ztw[k1*8 + j2] = w^{2 j2 k1}
   T2 *buf = ztw + N / 2;
-  T2 *stage = buf + G::PLANE_UNITS;  // 32 rows of N reals
+  T2 *stage = buf + P::UNITS;  // 32 rows of N reals
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
@@ -426,15 +436,15 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
-  const XgAreas<N, T> xa(p, rank);
+  const XgAreas<N, T, RW> xa(p, rank);
   const uint64_t spol = l2_stream_policy();  // streamed field data
-  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  const int cid = blockIdx.x / P::CL, ncl = gridDim.x / P::CL;
   const T *src = reinterpret_cast<const T *>(p.in[b]);
   T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
   auto issue = [&](int plane) {  // warp 0: one bulk copy per row of this CTA
-    if (lane == 0) mbar_expect_tx(bar, (unsigned)(kRows * N * sizeof(T)));
+    if (lane == 0) mbar_expect_tx(bar, (unsigned)(RW * N * sizeof(T)));
     __syncwarp();
-    bulk_g2s(stage + lane * (N / 2), src + ((size_t)plane * N + rank * kRows + lane) * N, N * sizeof(T), bar);
+    bulk_g2s(stage + lane * (N / 2), src + ((size_t)plane * N + rank * RW + lane) * N, N * sizeof(T), bar);
   };
   if (tid == 0) {
     mbar_init(bar, 1);
@@ -453,11 +463,11 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_fwd_kernel(const __grid_c
     const int next = plane + ncl;
     if (STAGED) mbar_wait(bar, it & 1, &s_err);
     // next plane's rows towards L2 while this one is transformed
-    if (!STAGED && next < N && tid < kRows)
-      prefetch_l2(src + ((size_t)next * N + rank * kRows + tid) * N, N * sizeof(T));
+    if (!STAGED && next < N && tid < RW)
+      prefetch_l2(src + ((size_t)next * N + rank * RW + tid) * N, N * sizeof(T));
     {
       const int j2 = tid & 7, r = tid >> 3;
-      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
       const T2 *row = STAGED ? stage + r * (N / 2) : reinterpret_cast<const T2 *>(src + rowoff);
       T2 v[N1];
       sfor<0, N1>([&](auto J1) {
@@ -730,18 +740,19 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
 //      __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
 // CPS as for plane_fwd: 1 stages the next plane's columns with a tensor copy,
 // 2 loads them straight from global memory (two CTAs per SM).
-template <int N, class T, class Epi, int CPS, int XG = 0>
-__global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_constant__ KParams p) {
+template <int N, class T, class Epi, int CPS, int XG = 0, int RW = kRows>
+__global__ void __launch_bounds__(8 * RW, CPS) plane_inv_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
-  using P = Plane<N, T>;
+  using P = Plane<N, T, RW>;
   constexpr int M = G::M;
   constexpr bool STAGED = (CPS == 1);
+  static_assert(!STAGED || RW == kRows, "the staged variant has 32-row CTAs");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
   T2 *ztw = tw + N;
   T2 *buf = ztw + N / 2;
-  T2 *stage = buf + G::PLANE_UNITS;  // [ky][16 columns]
+  T2 *stage = buf + P::UNITS;  // [ky][16 columns]
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
@@ -751,12 +762,12 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
-  const XgAreas<N, T> xa(p, rank);
+  const XgAreas<N, T, RW> xa(p, rank);
   const uint64_t spol = l2_stream_policy();  // streamed field data
-  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  const int cid = blockIdx.x / P::CL, ncl = gridDim.x / P::CL;
   auto issue = [&](int plane) {  // thread 0: one tensor box (this CTA's 16 columns x all ky)
     mbar_expect_tx(bar, (unsigned)(N * 16 * sizeof(T2)));
-    tma_load_3d(stage, &p.tmi[b], 2 * rank * kCols, 0, plane, bar);
+    tma_load_3d(stage, &p.tmi[b], 2 * rank * P::CW, 0, plane, bar);
   };
   if (tid == 0) {
     mbar_init(bar, 1);
@@ -777,13 +788,14 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     const int next = plane + ncl;
     if (STAGED) mbar_wait(bar, it & 1, &s_err);
     // next plane's columns towards L2 while this one is transformed
-    if (!STAGED && next < N && tid < N)
-      prefetch_l2(gsrc + ((size_t)next * N + tid) * M + rank * kCols, kCols * sizeof(T2));
+    if (!STAGED && next < N)
+      for (int i = tid; i < N; i += P::TH)
+        prefetch_l2(gsrc + ((size_t)next * N + i) * M + rank * P::CW, P::CW * sizeof(T2));
     P::template yi<(XG & kXgInv) != 0>(
         buf, tw, tid, cluster,
         [&](int ky, int c) -> T2 {
           return STAGED ? stage[ky * 16 + c]
-                        : ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c, spol);
+                        : ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * P::CW + c, spol);
         },
         xa.own[it & 1]);  // alternating areas, as in plane_fwd
     if (STAGED && tid == 0 && next < N) {
@@ -792,7 +804,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
     }
     P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[it & 1]);
     P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
-      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
       const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, acc);
       if (outb) reinterpret_cast<T2 *>(outb + rowoff)[j] = val;
     });
@@ -817,11 +829,11 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_kernel(const __grid_c
 // plane_inv, so the real field crosses HBM once per chain instead of twice per
 // step. Direct loads; CPS (2, 3 or 4) CTAs per SM, the layout of plane_fwd's
 // direct variant.
-template <int N, class T, class Epi, class Pro, int CPS, int XG = 0>
-__global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
+template <int N, class T, class Epi, class Pro, int CPS, int XG = 0, int RW = kRows>
+__global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
-  using P = Plane<N, T>;
+  using P = Plane<N, T, RW>;
   constexpr int M = G::M, N1 = G::N1;
   constexpr int NE = Epi::NR, NP = Pro::NR, NA = (NE + NP > 0) ? NE + NP : 1;
   static_assert(NA <= kRedMax, "reduction count");
@@ -829,7 +841,7 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
   T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
   T2 *ztw = tw + N;
   T2 *buf = ztw + N / 2;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(buf + G::PLANE_UNITS);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
   double *red = reinterpret_cast<double *>(bar + 2);
   if (flow_stopped(p)) return;
   // uniform over the grid: set by the pencil pass of this step, before launch
@@ -839,9 +851,9 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
   const int rank = (int)cluster.block_rank();
-  const XgAreas<N, T> xa(p, rank);
+  const XgAreas<N, T, RW> xa(p, rank);
   const uint64_t spol = l2_stream_policy();  // streamed field data
-  const int cid = blockIdx.x / G::CL, ncl = gridDim.x / G::CL;
+  const int cid = blockIdx.x / P::CL, ncl = gridDim.x / P::CL;
   plane_twiddles<N, T>(p, tw, ztw);
   double acc_e[NE > 0 ? NE : 1], acc_p[NP > 0 ? NP : 1];
 #pragma unroll
@@ -855,16 +867,17 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
 
   for (int plane = cid; plane < N; plane += ncl) {
     // next plane's columns towards L2 while this one is transformed
-    if (plane + ncl < N && tid < N)
-      prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + tid) * M + rank * kCols, kCols * sizeof(T2));
+    if (plane + ncl < N)
+      for (int i = tid; i < N; i += P::TH)
+        prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + i) * M + rank * P::CW, P::CW * sizeof(T2));
     P::template yi<(XG & kXgInv) != 0>(
         buf, tw, tid, cluster,
-        [&](int ky, int c) -> T2 { return ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * kCols + c, spol); },
+        [&](int ky, int c) -> T2 { return ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * P::CW + c, spol); },
         xa.own[0]);
     P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[0]);
     if (stop) {
       P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
-        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
         reinterpret_cast<T2 *>(phi + rowoff)[j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
       });
       // no forward exchange on this path: its barrier keeps the inverse areas
@@ -873,13 +886,13 @@ __global__ void __launch_bounds__(kThreads, CPS) plane_inv_fwd_kernel(const __gr
     } else {
       // phi rows [r][M] in buf (each warp writes and then reads its own rows)
       P::template zi2<true>(buf, tid, [&](int r, int j, T2 z) {
-        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
         buf[r * M + j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
       });
       __syncwarp();
       {
         const int j2 = tid & 7, r = tid >> 3;
-        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * kRows + r)) * N;
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
         T2 v[N1];
         sfor<0, N1>([&](auto J1) {
           constexpr int j1 = SPM_CI(J1);

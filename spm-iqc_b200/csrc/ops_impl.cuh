@@ -33,17 +33,27 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
 
 // Persistent cluster launch: as many clusters as can be resident at once
 // (queried once per kernel and device), at most one per x-plane.
-template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p,
-                                                               int nb, const char *what, bool xg = false) {
+template <class Tag, int N, class K, int RW = kRows>
+static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int nb, const char *what,
+                          bool xg = false) {
+  constexpr int CLr = N / RW;
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
+  if (e == cudaSuccess && CLr > 8) {  // clusters of up to 16 CTAs (16-row CTAs at N = 256)
+    static std::atomic<unsigned> np{0};
+    const int dev = c->device < 32 ? c->device : 0;
+    if (!((np.load(std::memory_order_acquire) >> dev) & 1u)) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e == cudaSuccess) np.fetch_or(1u << dev, std::memory_order_release);
+    }
+  }
   if (e != cudaSuccess) return spm_fail_cuda(e, what);
   cudaLaunchConfig_t cfg = {};
-  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.blockDim = dim3(8 * RW, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = c->stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = Geo<N>::CL;
+  at[0].val.clusterDim.x = CLr;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
@@ -54,16 +64,16 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
   const int dev = c->device < 32 ? c->device : 0;
   int nc = ncl[dev].load(std::memory_order_relaxed);
   if (nc == 0) {
-    cfg.gridDim = dim3(Geo<N>::CL * N, 1, 1);
+    cfg.gridDim = dim3(CLr * N, 1, 1);
     int n = 0;
     e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
     if (e != cudaSuccess || n < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, what);
     nc = n < N ? n : N;
     ncl[dev].store(nc, std::memory_order_relaxed);
   }
-  cfg.gridDim = dim3(Geo<N>::CL * nc, nb, 1);
+  cfg.gridDim = dim3(CLr * nc, nb, 1);
   // a kernel exchanging through global areas needs one per CTA (nb == 1)
-  if (xg && (!p.xg || nb != 1 || Geo<N>::CL * nc > p.xg_cap))
+  if (xg && (!p.xg || nb != 1 || CLr * nc > p.xg_cap * (kRows / RW)))
     return spm_fail(SPM_ERR_STATE, "plane exchange areas missing or too small");
   c->launches++;
   e = cudaLaunchKernelEx(&cfg, kern, p);
@@ -76,9 +86,13 @@ template <class Tag, int N, class K> static int launch_cluster(spm_ctx *c, K ker
 template <class X> struct XgOk : std::false_type {};
 template <class T> struct XgOk<ProGrad<T>> : std::true_type {};
 template <class T> struct XgOk<EpiFlow<T>> : std::true_type {};
-static inline int xg_bits(const spm_ctx *c, int nb) { return (c->xg && nb == 1 && c->plane_cps >= 2) ? c->plane_xg : 0; }
+// plane_cps 5: gradient chains with both exchanges through L2 run 16-row CTAs
+// (128 threads, four per SM, 128 registers each); other chains run as with 2.
+static inline int eff_cps(const spm_ctx *c) { return c->plane_cps == 5 ? 2 : c->plane_cps; }
+static inline int xg_bits(const spm_ctx *c, int nb) { return (c->xg && nb == 1 && eff_cps(c) >= 2) ? c->plane_xg : 0; }
+static inline bool rw16(const spm_ctx *c, int nb) { return c->plane_cps == 5 && xg_bits(c, nb) == (kXgFwd | kXgInv); }
 // Four CTAs per SM (64 registers per thread): FP32 gradient chains only.
-template <class T> static inline bool cps4(const spm_ctx *c) { return sizeof(T) == 4 && c->plane_cps == 4; }
+template <class T> static inline bool cps4(const spm_ctx *c) { return sizeof(T) == 4 && eff_cps(c) == 4; }
 
 // The plane kernels come in four variants (c->plane_cps): 1 = staged, one CTA
 // per SM; 2 = direct loads, two CTAs per SM; 3 = direct, three CTAs per SM;
@@ -86,6 +100,11 @@ template <class T> static inline bool cps4(const spm_ctx *c) { return sizeof(T) 
 template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KParams &p, int nb) {
   if constexpr (XgOk<Pro>::value) {
     if (xg_bits(c, nb) & kXgFwd) {
+      if (rw16(c, nb)) {
+        struct Tag16 {};
+        return launch_cluster<Tag16, N, decltype(&plane_fwd_kernel<N, T, Pro, 4, kXgFwd, 16>), 16>(
+            c, plane_fwd_kernel<N, T, Pro, 4, kXgFwd, 16>, plane_smem<N, T, 4, 16>(), p, nb, "plane_fwd", true);
+      }
       if constexpr (sizeof(T) == 4) {
         if (cps4<T>(c)) {
           struct Tag4x {};
@@ -93,7 +112,7 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
                                           "plane_fwd", true);
         }
       }
-      if (c->plane_cps >= 3) {
+      if (eff_cps(c) >= 3) {
         struct Tag3x {};
         return launch_cluster<Tag3x, N>(c, plane_fwd_kernel<N, T, Pro, 3, kXgFwd>, plane_smem<N, T, 3>(), p, nb,
                                         "plane_fwd", true);
@@ -103,11 +122,11 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
                                       "plane_fwd", true);
     }
   }
-  if (c->plane_cps >= 3) {
+  if (eff_cps(c) >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_fwd_kernel<N, T, Pro, 3>, plane_smem<N, T, 3>(), p, nb, "plane_fwd");
   }
-  if (c->plane_cps == 2) {
+  if (eff_cps(c) == 2) {
     struct Tag2 {};
     return launch_cluster<Tag2, N>(c, plane_fwd_kernel<N, T, Pro, 2>, plane_smem<N, T, 2>(), p, nb, "plane_fwd");
   }
@@ -117,6 +136,11 @@ template <int N, class T, class Pro> static int plane_fwd(spm_ctx *c, const KPar
 template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KParams &p0, int nb) {
   if constexpr (XgOk<Epi>::value) {
     if (xg_bits(c, nb) & kXgInv) {
+      if (rw16(c, nb)) {
+        struct Tag16 {};
+        return launch_cluster<Tag16, N, decltype(&plane_inv_kernel<N, T, Epi, 4, kXgInv, 16>), 16>(
+            c, plane_inv_kernel<N, T, Epi, 4, kXgInv, 16>, plane_smem<N, T, 4, 16>(), p0, nb, "plane_inv", true);
+      }
       if constexpr (sizeof(T) == 4) {
         if (cps4<T>(c)) {
           struct Tag4x {};
@@ -124,7 +148,7 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
                                           "plane_inv", true);
         }
       }
-      if (c->plane_cps >= 3) {
+      if (eff_cps(c) >= 3) {
         struct Tag3x {};
         return launch_cluster<Tag3x, N>(c, plane_inv_kernel<N, T, Epi, 3, kXgInv>, plane_smem<N, T, 3>(), p0, nb,
                                         "plane_inv", true);
@@ -134,11 +158,11 @@ template <int N, class T, class Epi> static int plane_inv(spm_ctx *c, const KPar
                                       "plane_inv", true);
     }
   }
-  if (c->plane_cps >= 3) {
+  if (eff_cps(c) >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_inv_kernel<N, T, Epi, 3>, plane_smem<N, T, 3>(), p0, nb, "plane_inv");
   }
-  if (c->plane_cps == 2) {
+  if (eff_cps(c) == 2) {
     struct Tag2 {};
     return launch_cluster<Tag2, N>(c, plane_inv_kernel<N, T, Epi, 2>, plane_smem<N, T, 2>(), p0, nb, "plane_inv");
   }
@@ -158,7 +182,7 @@ static int plane_inv_fwd_xg(spm_ctx *c, const KParams &p, int nb) {
                                      "plane_inv_fwd", true);
     }
   }
-  if (c->plane_cps >= 3) {
+  if (eff_cps(c) >= 3) {
     struct Tag3 {};
     return launch_cluster<Tag3, N>(c, plane_inv_fwd_kernel<N, T, Epi, Pro, 3, XG>, plane_smem<N, T, 3>(), p, nb,
                                    "plane_inv_fwd", XG != 0);
@@ -169,6 +193,12 @@ static int plane_inv_fwd_xg(spm_ctx *c, const KParams &p, int nb) {
 }
 template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
   if constexpr (XgOk<Pro>::value && XgOk<Epi>::value) {
+    if (rw16(c, nb)) {
+      struct Tag16 {};
+      constexpr int XG = kXgFwd | kXgInv;
+      return launch_cluster<Tag16, N, decltype(&plane_inv_fwd_kernel<N, T, Epi, Pro, 4, XG, 16>), 16>(
+          c, plane_inv_fwd_kernel<N, T, Epi, Pro, 4, XG, 16>, plane_smem<N, T, 4, 16>(), p, nb, "plane_inv_fwd", true);
+    }
     switch (xg_bits(c, nb)) {
       case kXgFwd: return plane_inv_fwd_xg<N, T, Epi, Pro, kXgFwd>(c, p, nb);
       case kXgInv: return plane_inv_fwd_xg<N, T, Epi, Pro, kXgInv>(c, p, nb);

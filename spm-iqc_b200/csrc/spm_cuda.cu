@@ -332,7 +332,7 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
 extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
   if (!c || !knob) return spm_fail(SPM_ERR_ARG, "null argument");
   if (std::strcmp(knob, "plane_cps") == 0) {
-    if (value < 1 || value > 4) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1, 2, 3 or 4");
+    if (value < 1 || value > 5) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1 to 5");
     c->plane_cps = value;
     return SPM_OK;
   }
