@@ -90,7 +90,7 @@ const char *spm_status_str(int status);
  * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
  * inverse plane pass with the next step's forward one (phi stays on chip
  * between steps; the same bits as 0), 0 = three passes per step.
- * knob "plane_xg" (0..3, plane_cps 2 to 4): the plane kernels of
+ * knob "plane_xg" (0..3, plane_cps 2 to 5): the plane kernels of
  * gradient chains exchange the x-plane between the CTAs of a cluster through
  * distributed shared memory (0) or through per-CTA areas in global memory that
  * stay resident in L2 (bit 1: the forward exchange, bit 2: the inverse one;
