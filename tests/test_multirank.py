@@ -72,3 +72,18 @@ def test_two_rank_paths_on_gloo():
     specs = workloads.serving_stream(5, 24, rate=50.0, sizes=(32, 64))
     loads = [sum(workloads.job_bytes(specs[i]) for i in p) for p in out[0][2]]
     assert max(loads) <= 1.3 * min(loads)
+
+
+def test_bench_reads_the_committed_traffic_profile():
+    """bench.py's roofline.traffic comes from the committed ncu summary: every
+    chain kernel of the gradient step has a per-launch byte count there, and the
+    fused plane pass and the pencil pass move no more than 10 % above their
+    algorithmic bytes (no re-reads)."""
+    import sys
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "spm-iqc_b200")]
+    import bench
+    tr = bench.kernel_traffic()
+    S = 256 ** 3 * 8
+    assert set(tr) == {"pencil<OpGrad>", "plane_inv_fwd<EpiFlow,ProGrad>", "plane_fwd<ProGrad>", "plane_inv<EpiFlow>"}
+    assert 0 < tr["pencil<OpGrad>"] <= 1.1 * 4 * S
+    assert 0 < tr["plane_inv_fwd<EpiFlow,ProGrad>"] <= 1.1 * 2 * S
