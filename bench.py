@@ -376,6 +376,21 @@ def solver_legs(ctx, phi):
     import torch
     solvers = {}
     try:
+        # the building blocks: my_fft, my_ifft, ngrad_cam (one call each, 20 times)
+        uh = ctx.my_fft(phi)
+        back = torch.empty_like(phi)
+        grad = torch.empty_like(phi)
+        ctx.my_ifft(uh, back)
+        ctx.ngrad_cam(phi, grad)
+        for name, fn in (("my_fft", lambda: ctx.my_fft(phi, uh)), ("my_ifft", lambda: ctx.my_ifft(uh, back)),
+                         ("ngrad_cam", lambda: ctx.ngrad_cam(phi, grad))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(20):
+                fn()
+            torch.cuda.synchronize()
+            solvers[name + "_per_s"] = 20 / (time.perf_counter() - t0)
+        del uh, back, grad
         Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
         ctx.hiosd_lobpcg_inip(phi, Vb, maxiter=2)
         Vb = ctx.hiosd_lobpcg_initialization(8, seed=3)
