@@ -291,7 +291,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
-// dst/src 16-byte aligned, bytes a multiple of 16.
+// One 16-byte global -> shared copy that bypasses registers and L1
+// (both addresses 16-byte aligned); completes at cp_async_wait_all(), or
+// by commit groups.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)),
+               "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// all but the most recently committed group complete
+__device__ __forceinline__ void cp_async_wait_all_but_last() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
 // Asks for `bytes` at src (16-byte aligned, a multiple of 16) to be brought
 // into L2; no registers, shared memory or completion tracking involved.
 __device__ __forceinline__ void prefetch_l2(const void *src, unsigned bytes) {

@@ -47,9 +47,22 @@ template <int N, class T, int CPS, int RW = kRows> constexpr size_t plane_smem()
 // Pencil symbol table (per tile): 9 kz rows (the tile's 8 columns and kz = N/2)
 // x |Kx| = 0..N/2, one double2 half of the K^2 symbols each.
 template <int N> constexpr int pencil_sym_entries() { return 9 * (N / 2 + 1); }
-template <int N, class T> constexpr size_t pencil_smem(int stages, bool sym) {
+template <int N, class T> constexpr size_t pencil_smem_n(int stages, int symbufs) {
   return sizeof(c2<T>) * (N + Geo<N>::PENCIL_UNITS + (size_t)stages * Geo<N>::STAGE_UNITS) + 16 +
-         sizeof(double) * 32 * kRedMax + (sym ? sizeof(double2) * pencil_sym_entries<N>() : 0) + 128;
+         sizeof(double) * 32 * kRedMax + sizeof(double2) * pencil_sym_entries<N>() * symbufs + 128;
+}
+// CTAs of `smem` bytes that one SM holds (228 KB per SM, 1 KB reserved per CTA,
+// at most 227 KB per CTA).
+constexpr int smem_ctas_per_sm(size_t smem) { return smem > 232448 ? 0 : (int)(233472 / (smem + 1024)); }
+// Symbol buffers of the pencil: two (the next tile's copies start a whole
+// tile ahead) where the second one costs no resident CTA, else one.
+template <int N, class T> constexpr int pencil_sym_bufs(int stages, bool sym) {
+  return !sym ? 0
+         : smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 2)) == smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 1)) ? 2
+                                                                                                               : 1;
+}
+template <int N, class T> constexpr size_t pencil_smem(int stages, bool sym) {
+  return pencil_smem_n<N, T>(stages, pencil_sym_bufs<N, T>(stages, sym));
 }
 
 __device__ __forceinline__ unsigned char *smem_base128(unsigned char *raw) {
@@ -538,24 +551,30 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
   constexpr int NCH = M / 8;
   // Symbols: a tile's points have |Ky| = t (rows t and N - t, t > 0), Kz in
   // its 8 columns (or N/2 for the packed c = 0 column) and any Kx, so the
-  // 9 x (N/2 + 1) entries it needs are staged in shared memory, fetched into
-  // registers one tile ahead (the table lookups of every point would
-  // otherwise wait on L2). Tiles with t = 0 (rows 0 and N/2) read the table.
+  // 9 x (N/2 + 1) entries it needs are staged in shared memory (the table
+  // lookups of every point would otherwise wait on L2). The copies are
+  // asynchronous, awaited just before the tile's point operator; with two
+  // buffers they start at the top of the previous tile, with one once the
+  // previous tile's point operator is done. Tiles with t = 0 (rows 0 and
+  // N/2) read the table.
   constexpr bool USE_SYM = Op::SYM >= 0;
   constexpr int KXS = N / 2 + 1, SYMN = pencil_sym_entries<N>();
-  constexpr int SPT = USE_SYM ? (SYMN + kThreads - 1) / kThreads : 1;
-  double2 pre[SPT];
-  auto sym_fetch = [&](int tl) {
+  constexpr int SYMB = pencil_sym_bufs<N, T>(NST, USE_SYM);
+  auto sym_stage = [&](int tl, double2 *dst) {
     const int tt = tl / NCH, cz = (tl % NCH) * 8;
-#pragma unroll
-    for (int i = 0; i < SPT; i++) {
-      const int e = tid + i * kThreads;
-      if (e < SYMN) {
-        const int row = e / KXS, a = e - row * KXS;
-        const int kz = row < 8 ? cz + row : N / 2;
-        pre[i] = symbols_half(p, a * a + tt * tt + kz * kz, USE_SYM ? Op::SYM : 0);
-      }
+    const double2 *g = reinterpret_cast<const double2 *>(p.gtab) + (USE_SYM ? Op::SYM : 0);
+    for (int e = tid; e < SYMN; e += kThreads) {
+      const int row = e / KXS, a = e - row * KXS;
+      const int kz = row < 8 ? cz + row : N / 2;
+      cp_async16(dst + e, g + 2 * (a * a + tt * tt + kz * kz));
     }
+  };
+  // this tile's copies complete (with two buffers the next tile's may not)
+  auto sym_wait = [&]() {
+    if constexpr (SYMB == 2)
+      cp_async_wait_all_but_last();
+    else
+      cp_async_wait_all();
   };
   // thread 0: two tensor boxes (8 columns x all x) for rows ky0, ky1 of a tile
   auto issue = [&](const CUtensorMap *map, T2 *dst, uint64_t *bar, int tile) {
@@ -581,8 +600,10 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
     if (Op::FI) issue(&p.tmi[b], sA, &bars[0], tile);
     if (Op::SI) issue(&p.tms[b], sS, &bars[1], tile);
   }
-  if constexpr (USE_SYM)
-    if (tile < G::PTILES && tile / NCH != 0) sym_fetch(tile);
+  if constexpr (USE_SYM) {
+    if (tile < G::PTILES && tile / NCH != 0) sym_stage(tile, stab);
+    if constexpr (SYMB == 2) cp_async_commit();
+  }
 
   for (int it = 0; tile < G::PTILES; tile += gridDim.x, it++) {
     const int next = tile + gridDim.x;
@@ -592,22 +613,22 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
     const int ky = rowsel ? ky1 : ky0;
     const int col = c0 + cc;
     const bool dc = (c0 == 0);
-    if constexpr (USE_SYM) {
-      // the previous tile's point operator is done (barrier at the loop end)
-      if (t != 0) {
-#pragma unroll
-        for (int i = 0; i < SPT; i++)
-          if (tid + i * kThreads < SYMN) stab[tid + i * kThreads] = pre[i];
-      }
-      if (next < G::PTILES && next / NCH != 0) sym_fetch(next);
-      if constexpr (!Op::FI) __syncthreads();
+    double2 *const sym_cur = stab + (SYMB == 2 ? (it & 1) * SYMN : 0);
+    if constexpr (SYMB == 2) {
+      // the other buffer's tile (two back) finished its point operator
+      if (next < G::PTILES && next / NCH != 0) sym_stage(next, stab + ((it + 1) & 1) * SYMN);
+      cp_async_commit();
+    }
+    if constexpr (USE_SYM && !Op::FI) {
+      sym_wait();
+      __syncthreads();
     }
     // symbols of (Kx, Ky, Kz) for kz row `row` of the tile (8: kz = N/2)
     auto sym_at = [&](int Kx, int Ky, int Kz, int row) -> double2 {
       if constexpr (!USE_SYM) {
         return double2{0.0, 0.0};
       } else {
-        if (t != 0) return stab[row * KXS + (Kx < 0 ? -Kx : Kx)];
+        if (t != 0) return sym_cur[row * KXS + (Kx < 0 ? -Kx : Kx)];
         return symbols_half(p, Kx * Kx + Ky * Ky + Kz * Kz, Op::SYM);
       }
     };
@@ -628,6 +649,7 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
           ex[kk * 256 + j2 * 16 + pen] = (kk == 0) ? v[kk] : cmul(v[kk], tw[j2 * kk]);
         });
       }
+      if constexpr (USE_SYM) sym_wait();  // this tile's symbols, seen after the barrier
       __syncthreads();
       if (tid == 0 && next < G::PTILES) {
         fence_proxy_async();
@@ -694,13 +716,15 @@ __global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_consta
         F[k2] = o_inv;
       }
     }
-    __syncthreads();  // sS and ex reads done
+    __syncthreads();  // sS, stab and ex reads done
     if constexpr (Op::SI) {
       if (tid == 0 && next < G::PTILES) {
         fence_proxy_async();
         issue(&p.tms[b], sS, &bars[1], next);
       }
     }
+    if constexpr (SYMB == 1)
+      if (next < G::PTILES && next / NCH != 0) sym_stage(next, stab);
     if constexpr (Op::INV) {
       if (has2) {
         Dft<+1, 16, T2>::run(F);  // over k2 -> j2
