@@ -61,6 +61,14 @@ template <int N, class T> constexpr int pencil_sym_bufs(int stages, bool sym) {
          : smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 2)) == smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 1)) ? 2
                                                                                                                : 1;
 }
+// Resident pencil CTAs per SM the registers are budgeted for: two for FP32
+// pencils whose shared memory (one symbol buffer) lets two CTAs of 256
+// threads share an SM, which bounds them to 128 registers a thread; else one.
+// (At 256^3 FP32 the gradient pencil does not fit twice: one CTA with two
+// symbol buffers beat two CTAs with one buffer each.)
+template <int N, class T> constexpr int pencil_min_ctas(int stages, bool sym) {
+  return sizeof(T) == 4 && smem_ctas_per_sm(pencil_smem_n<N, T>(stages, sym ? 1 : 0)) >= 2 ? 2 : 1;
+}
 template <int N, class T> constexpr size_t pencil_smem(int stages, bool sym) {
   return pencil_smem_n<N, T>(stages, pencil_sym_bufs<N, T>(stages, sym));
 }
@@ -524,7 +532,8 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
 //     __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
 // Stages: [A (if FI)][S (if SI)], each 2 rows x N x 8 columns, [row][x][cc].
 template <int N, class T, class Op>
-__global__ void __launch_bounds__(kThreads, 1) pencil_kernel(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0))
+    pencil_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
   using T2 = c2<T>;
   constexpr int M = G::M, M1 = G::M1;
