@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
   T2 *sS = sA + (Op::FI ? G::STAGE_UNITS : 0);
   uint64_t *bars = reinterpret_cast<uint64_t *>(ex + G::PENCIL_UNITS + NST * G::STAGE_UNITS);
   double *red = reinterpret_cast<double *>(bars + 2);
-  double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbols of the current tile
+  double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbol buffers (one or two tiles)
   __shared__ int s_err;
   if (flow_stopped(p)) return;
 
