@@ -217,6 +217,7 @@ template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams 
   }
   auto kern = pencil_kernel<N, T, Op>;
   constexpr size_t smem = pencil_smem<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0);
+  static_assert(smem_ctas_per_sm(smem) >= 1, "pencil shared memory above the 227 KB a CTA may use");
   struct Tag {};
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e != cudaSuccess) return spm_fail_cuda(e, "pencil attribute");
