@@ -1,5 +1,5 @@
 """CUDA path vs the FP64 oracle: transforms, energy, gradient flow, ngrad, Hv,
-preconditioner, inner products. Tolerance: the north-star FP64 bar, 1e-11
+preconditioner, inner products. Tolerance: the FP64 parity bar, 1e-11
 relative (scale-relative max difference for fields)."""
 import numpy as np
 import pytest

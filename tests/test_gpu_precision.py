@@ -2,7 +2,7 @@
 against FP64: an FP32 gradient step is within 1e-5 (scale-relative) of the
 FP64 oracle; the mixed flow (FP32 to a switch threshold, FP64 polish) reaches
 ||grad F|| <= 1e-8 with the energy within 1e-10 relative of the all-FP64 GPU
-flow."""
+flow (the mixed-precision acceptance bar)."""
 import numpy as np
 import pytest
 
