@@ -182,6 +182,93 @@ def cpu_reference_steps(phi, budget_s: float, max_steps: int, warm: int = 1):
     return n / dt, threads, n, dt
 
 
+def cpu_legs(ctx, phi_h, budget_s: float = 20.0, n_parity: int = 3, max_timed: int = 10):
+    """The CPU side of the benchmark, on the same 256^3 workload and phi0:
+
+    * parity: the reference's own get_min_u_F (compiled here, one rank) runs
+      n_parity steps that record E, res and ||grad F|| per step, then up to
+      max_timed plain iterations (timed: cpu_baseline); the GPU context the
+      benchmark times (its autotuned schedule) runs the same number of steps
+      from the same phi0, and the records, the final phi and u, and the final
+      energy and ||grad F|| are compared (the FP64 bar is 1e-11 relative);
+    * the same reference on one host thread (a bounded sample);
+    * an FFTW-class arm: the step restated over torch's CPU FFT (MKL) on all
+      host threads (oracle/cpu_mkl.py), the reference planning FFTW with
+      FFTW_PATIENT (My_FFT.cpp:70-85) where this image has no FFTW.
+    Returns (cpu_baseline, parity, serial, mkl)."""
+    import numpy as np
+    import torch
+    from oracle import refbind
+    threads = os.cpu_count() or 1
+    r = refbind.Ref(N, L, TAU, GAMMA, DT, threads=threads)
+    r.set_state(phi_h)
+    E, res, g = r.grad_steps(n_parity)
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_timed and (time.perf_counter() - t0) < budget_s:
+        r.get_min_u_F(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    cpu = {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "reference",
+           "sample": f"{n} full 256^3 steps in {dt:.1f} s after {n_parity} recorded steps (reference src/*.cpp "
+                     f"compiled unchanged, project FFT shim on {threads} threads)"}
+    p_ref, u_ref = r.get_state()
+    E_end = r.energy()
+    g_end = float(np.sqrt(np.mean(r.ngrad(p_ref) ** 2)))
+    # one host thread: a bounded sample of the same loop
+    r.set_threads(1)
+    t0 = time.perf_counter()
+    ns = 0
+    while ns < 3 and (ns == 0 or (time.perf_counter() - t0) < 0.5 * budget_s):
+        r.get_min_u_F(1)
+        ns += 1
+    dts = time.perf_counter() - t0
+    r.close()
+    serial = {"value": ns / dts, "unit": "steps/s", "cores": 1, "kind": "reference",
+              "sample": f"{ns} full 256^3 steps in {dts:.1f} s, shim FFT on one thread"}
+    total = n_parity + n
+    phi = torch.from_numpy(phi_h.copy()).cuda()
+    uh = ctx.my_fft(phi)
+    st = ctx.get_min_u_F(phi, uh, total)
+    E_gpu, g_gpu = ctx.get_Ene(phi, uh), ctx.ngrad_cam(phi)[1]
+    pg, ug = phi.cpu().numpy(), ctx.to_full(uh).cpu().numpy()
+
+    def srel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    parity = {"steps": total, "schedule": ctx.tuning(),
+              "per_step_max_rel_dE": float(np.max(np.abs(st[:n_parity, 0] - E) / np.abs(E))),
+              "per_step_max_rel_dgrad": float(np.max(np.abs(st[:n_parity, 2] - g) / np.abs(g))),
+              "per_step_max_rel_dres": float(np.max(np.abs(st[:n_parity, 1] - res) / np.abs(res))),
+              "final_rel_dE": abs(E_gpu - E_end) / abs(E_end), "final_rel_dgrad": abs(g_gpu - g_end) / g_end,
+              "phi_scale_rel_diff": srel(pg, p_ref), "u_scale_rel_diff": srel(ug, u_ref), "bar": 1e-11}
+    parity["pass"] = all(parity[k] <= 1e-11 for k in ("per_step_max_rel_dE", "per_step_max_rel_dgrad",
+                                                          "final_rel_dE", "final_rel_dgrad", "phi_scale_rel_diff",
+                                                          "u_scale_rel_diff"))
+    del phi, uh
+    mkl = mkl_arm(phi_h, budget_s=0.5 * budget_s, max_steps=20, threads=threads)
+    return cpu, parity, serial, mkl
+
+
+def mkl_arm(phi_h, budget_s: float, max_steps: int, threads: int):
+    """The gradient step over torch's CPU FFT (MKL): one warm-up step, then
+    timed steps until budget_s or max_steps."""
+    import torch
+    from oracle import cpu_mkl
+    f = cpu_mkl.MklFlow(N, L, TAU, GAMMA, DT, threads=threads)
+    p = torch.from_numpy(phi_h.copy())
+    u = f.spectrum(p)
+    p, u, *_ = f.step(p, u)
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        p, u, *_ = f.step(p, u)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "steps/s", "cores": f.threads, "kind": "port",
+            "sample": f"{n} full 256^3 steps in {dt:.1f} s: the step (E, res, ||grad F||, one R2C and one C2R "
+                      f"transform) restated over torch.fft on the CPU (Intel MKL), {f.threads} threads"}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -196,11 +283,16 @@ def reference_arm(args, rank, world):
     sample = (f"{n} of the requested {args.steps} steps (each step the full 256^3 workload), "
               f"{dt:.1f} s, after {warm} warm-up step(s); reference src/*.cpp compiled unchanged with the "
               f"project FFT shim on {cores} threads")
+    try:  # the same step over an FFTW-class library FFT, beside the shimmed reference
+        mkl = mkl_arm(phi, budget_s=15.0, max_steps=max(args.steps, 1), threads=cores)
+    except Exception as ex:
+        mkl = {"value": None, "sample": f"unavailable: {ex}"}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
             "steps": n, "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "N": N},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "reference", "sample": sample},
+            "cpu_baseline_mkl": mkl,
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -427,8 +519,11 @@ def solvers_bench(args):
     import spmiqc
     rank, world, local = dist_setup()
     torch.cuda.set_device(local)
-    ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp64")
-    phi = torch.from_numpy(initial_field(1 + rank)).cuda()
+    n = args.solvers_n
+    ctx = spmiqc.SpmContext(n, L, TAU, GAMMA, DT, "fp64")
+    import inputs
+    phi = torch.from_numpy(inputs.cosine_shell(n, inputs.icosahedral_shell(), amp=0.15, seed=1 + rank,
+                                               noise=1e-3)).cuda()
     uh = ctx.my_fft(phi)
     ctx.get_min_u_F(phi, uh, 100)
     out = solver_legs(ctx, phi)
@@ -437,9 +532,9 @@ def solvers_bench(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps({"metric": "LOBPCG k=8 iterations/s and SPM iterations/s (256^3 FP64)",
-                          "solvers_256_fp64": out, "n_gpus": world, "data": "synthetic",
-                          "config": {"workload": "bench field after 100 gradient steps", "N": N}}))
+        print(json.dumps({"metric": f"LOBPCG k=8 iterations/s and SPM iterations/s ({n}^3 FP64)",
+                          f"solvers_{n}_fp64": out, "n_gpus": world, "data": "synthetic",
+                          "config": {"workload": "bench field after 100 gradient steps", "N": n}}))
     return 0
 
 
@@ -463,6 +558,7 @@ def main():
     ap.add_argument("--batch-n", type=int, default=24)
     ap.add_argument("--solvers", action="store_true", help="run only the LOBPCG and SPM legs (one JSON line)")
     ap.add_argument("--batch-steps", type=int, default=4000)
+    ap.add_argument("--solvers-n", type=int, default=N, help="grid size of --solvers (small cases for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.serve:
@@ -670,13 +766,10 @@ def main():
     e2e_call = {"value": world * nd.value / call_s, "unit": "steps/s", "steps_per_call": nd.value,
                 "h2d_bytes_per_step": S / K, "d2h_bytes_per_step": (S + 32 * K) / K}
 
-    cpu = None
+    cpu = parity = cpu_serial = cpu_mkl = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            v, cores, n, dt = cpu_reference_steps(phi_h, budget_s=20.0, max_steps=10, warm=1)
-            cpu = {"value": v, "unit": "steps/s", "cores": cores, "kind": "reference",
-                   "sample": f"{n} full 256^3 steps in {dt:.1f} s (reference src/*.cpp compiled unchanged, "
-                             f"project FFT shim on {cores} threads)"}
+            cpu, parity, cpu_serial, cpu_mkl = cpu_legs(ctx, phi_h)
         except Exception as ex:  # oracle not built on this box
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {ex}"}
@@ -702,6 +795,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": S, "d2h_bytes_per_step": S + 32},
             "e2e_per_call": e2e_call,
             "cpu_baseline": cpu,
+            "cpu_baseline_serial": cpu_serial,
+            "cpu_baseline_mkl": cpu_mkl,
+            "parity": parity,
         }
         print(json.dumps(line))
     ctx.close()

@@ -112,6 +112,16 @@ int spm_autotune(spm_ctx *ctx, int steps, int *plane_cps, int *fuse_planes);
 const char *spm_last_error(void);
 /* Number of transform-kernel launches issued by this context so far. */
 uint64_t spm_launch_count(const spm_ctx *ctx);
+/* Failure-path self-test (no counterpart in the reference, which has no
+ * device code): launches one CTA whose mbarrier wait cannot complete (an
+ * arrival expecting 16 bytes with no copy issued) and gives it a limit of
+ * `polls` polls of ~256 ns (1 <= polls <= 2^22, the limit every transform
+ * kernel's waits use). The wait gives up, sets the context's error word and
+ * the kernel returns; the call synchronises the stream and returns what every
+ * entry point returns after such a timeout: SPM_ERR_CUDA with the message "a
+ * kernel's bounded wait for its asynchronous copies timed out". The error
+ * word is cleared by that read and the context stays usable. */
+int spm_selftest_bounded_wait(spm_ctx *ctx, int polls);
 
 /* ------------------------------------------------------------- transforms */
 
@@ -268,8 +278,11 @@ int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
  * nb is limited to 16 (SPM_ERR_ARG above): the reduction's scratch is a fixed
  * ~77 KB array in the library's device memory, resident on every device that
  * loads the library until exit. Calls share that array: calls that overlap on
- * the GPU race and must be ordered. The first call on a device looks up the
- * array's address; make it before any stream capture begins. */
+ * the GPU race and must be ordered. The stream and the pointers must belong to
+ * the device that is current at the call. The first call on a device looks up
+ * the array's address and keeps it; make it before any stream capture begins,
+ * and do not call this entry point on a device after a cudaDeviceReset (the
+ * array may then have moved). */
 int spm_inpfp_batch_noalloc(size_t n, int nb, int precision, const void *p, const void *q,
                             double *out, void *stream);
 

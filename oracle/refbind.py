@@ -17,7 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libspmref.so")
 # the same harness with the hot-path routines resolved to the GPU compat layer
 COMPAT_LIB = os.path.join(HERE, "_ref", "libspmref_compat.so")
-REFDIR_DEFAULT = "/root/reference"
+# The reference checkout: $SPMIQC_REFERENCE, else a directory named
+# "reference" beside this repository.
+REFDIR_DEFAULT = os.environ.get("SPMIQC_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                    "reference")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _libs = {}
@@ -86,6 +89,10 @@ class Ref:
         self.L.ref_set_threads(int(threads))
         if self.L.ref_setup(N, L, Tau, Gamma, dt) != 0:
             raise ValueError("ref_setup failed")
+
+    def set_threads(self, n):
+        """Host threads of the shim FFT (1: serial)."""
+        self.L.ref_set_threads(int(n))
 
     def _z(self, k=1):
         return np.zeros((k, self.N, self.N, self.N)) if k > 1 else np.zeros((self.N,) * 3)

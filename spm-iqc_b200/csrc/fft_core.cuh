@@ -395,15 +395,19 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 constexpr long kSpinLimit = 4L << 20;  // polls of ~256 ns: about 1 s
-// Returns false (and sets *err) when the phase did not complete in time.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+// Returns false (and sets *err) when the phase did not complete within
+// `limit` polls.
+__device__ __forceinline__ bool mbar_wait_n(uint64_t *bar, unsigned parity, int *err, long limit) {
   if (*((volatile int *)err)) return false;
-  for (long i = 0; i < kSpinLimit; i++) {
+  for (long i = 0; i < limit; i++) {
     if (mbar_try_wait(bar, parity)) return true;
     if (i > 16) __nanosleep(256);
   }
   atomicExch(err, 1);
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+  return mbar_wait_n(bar, parity, err, kSpinLimit);
 }
 
 // ------------------------------------------------------------------ parameters

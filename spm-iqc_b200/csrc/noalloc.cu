@@ -14,13 +14,19 @@
 //    rejected with SPM_ERR_ARG before anything is enqueued;
 //  * the scratch is one array per device, shared by every call on that device
 //    and holding whatever the previous call left in it; the tickets are cleared
-//    (cudaMemsetAsync) at the start of each call, the partials are always
-//    written before they are read;
+//    by the cudaMemsetAsync that each call enqueues ahead of its kernel (that
+//    clear is what later calls rely on, also after a kernel that was aborted
+//    half way), and the partials are always written before they are read;
+//  * the stream and the pointers must belong to the device that is current
+//    when the call is made: the scratch address is looked up for that device;
 //  * two calls whose kernels overlap on the GPU (different streams, no ordering
 //    between them) race on the scratch and give wrong results; order them;
 //  * the first call on each device looks up the device address of the scratch
-//    (cudaGetSymbolAddress, with that device current). Make that first call
-//    before any stream capture begins.
+//    (cudaGetSymbolAddress, with that device current) and keeps it for the
+//    life of the process. Make that first call before any stream capture
+//    begins. After a cudaDeviceReset (or any teardown of the device's primary
+//    context) the array may live at another address: do not use this entry
+//    point on that device afterwards.
 // The array stays resident on every device that loads this library until the
 // process exits (about 77 KB).
 #include <cuda_runtime.h>
@@ -71,10 +77,7 @@ __global__ void __launch_bounds__(kNoAllocThreads)
   double t[1] = {0.0};
   for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t[0] += __ldcg(partials + i);
   spm::block_reduce<1, 0u>(t, red);
-  if (threadIdx.x == 0) {
-    out[b] = t[0] * inv_n;
-    *ticket = 0u;
-  }
+  if (threadIdx.x == 0) out[b] = t[0] * inv_n;
 }
 
 int scratch_address(void **addr) {

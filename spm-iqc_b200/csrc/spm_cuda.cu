@@ -200,6 +200,37 @@ int spm_check_device_error(spm_ctx *c) {
   return SPM_OK;
 }
 
+// The failure path of the bounded waits, run on purpose: one thread arrives
+// on an mbarrier expecting 16 bytes of transactions and no copy is issued, so
+// the phase cannot complete; the wait gives up after `polls` polls, the CTA
+// reports through the context's error word and returns. Nothing is in flight
+// when it returns (no copy was issued), so the context stays usable.
+static __global__ void bounded_wait_selftest_kernel(int *err, long polls) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_err;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    s_err = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);
+  __syncthreads();
+  mbar_wait_n(&bar, 0, &s_err, polls);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_err) atomicExch(err, 1);
+}
+
+extern "C" int spm_selftest_bounded_wait(spm_ctx *c, int polls) {
+  if (!c || polls < 1 || polls > (int)kSpinLimit) return spm_fail(SPM_ERR_ARG, "polls must be in [1, 2^22]");
+  c->launches++;
+  bounded_wait_selftest_kernel<<<1, 32, 0, c->stream>>>(c->flow + FW_ERR, (long)polls);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return spm_fail_cuda(e, "bounded-wait self-test");
+  return spm_check_device_error(c);
+}
+
 int spm_read_scal(spm_ctx *c, int nb) {
   cudaError_t e = cudaMemcpyAsync(c->host_scal, c->scal, sizeof(double) * kScal * nb, cudaMemcpyDeviceToHost,
                                   c->stream);

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libspmiqc_cuda.so")
 
 SPM_FP64, SPM_FP32, SPM_MIXED = 0, 1, 2
 SPM_JOB_RELAX, SPM_JOB_LOBPCG, SPM_JOB_SPM = 0, 1, 2
-SPM_ERR_NOMEM, SPM_ERR_STATE, SPM_ERR_CANCELLED = 3, 6, 7
+SPM_ERR_ARG, SPM_ERR_CUDA, SPM_ERR_NOMEM, SPM_ERR_STATE, SPM_ERR_CANCELLED = 1, 2, 3, 6, 7
 _vp = ctypes.c_void_p
 _lib = None
 

@@ -55,6 +55,25 @@ def test_numpy_oracle_matches_reference_golden(N, steps):
     assert rel(ritz, GOLD[f"N{N}_ritz"]) < 1e-11
 
 
+@pytest.mark.parametrize("N,steps", [(16, 20), (32, 10)])
+def test_mkl_cpu_baseline_matches_reference_golden(N, steps):
+    """The FFTW-class CPU baseline (torch/MKL restatement of the gradient step)
+    reproduces the compiled reference's per-step energy, res and ||grad F||."""
+    import torch
+    from oracle import cpu_mkl
+    f = cpu_mkl.MklFlow(N, threads=2)
+    p = torch.from_numpy(npo.uniform_field(N, 7))
+    u = f.spectrum(p)
+    for s in range(steps):
+        p, u, e, r, g = f.step(p, u)
+        assert abs(e - GOLD[f"N{N}_E"][s]) <= 1e-12 * abs(e)
+        assert abs(r - GOLD[f"N{N}_res"][s]) <= 1e-10 * abs(r)
+        assert abs(g - GOLD[f"N{N}_gnorm"][s]) <= 1e-12 * abs(g)
+    ref = GOLD[f"N{N}_phi_end"] if N == 16 else GOLD[f"N{N}_phi_end_sig"]
+    got = p.numpy() if N == 16 else sig(p.numpy())
+    assert rel(got, ref) < 1e-12
+
+
 @pytest.mark.skipif(not refbind.available(), reason="oracle/_ref not built")
 def test_compiled_reference_matches_numpy():
     N = 16

@@ -45,6 +45,24 @@ def test_noalloc_inner_products_match(cuda):
     spmiqc.check(f(n, nb, spmiqc.SPM_FP32, P32.data_ptr(), Q32.data_ptr(), out.data_ptr(), stream))
     exp = (P32.double() * Q32.double()).reshape(nb, -1).sum(1).cpu().numpy() / n
     assert np.allclose(out.cpu().numpy(), exp, rtol=1e-12, atol=0)
+    # ragged sizes (fewer blocks than the scratch holds, one partial per block)
+    # with all 16 ticket slots in use, two calls enqueued back to back on one
+    # stream with no host synchronisation between them: the second call relies
+    # only on its own ticket clear, in stream order
+    for n_small in (1, 255, 1000):
+        A = cuda.from_numpy(np.stack([npo.uniform_field(16, 700 + b, amp=1.0).ravel()[:n_small]
+                                      for b in range(16)])).cuda()
+        B = cuda.from_numpy(np.stack([npo.uniform_field(16, 800 + b, amp=1.0).ravel()[:n_small]
+                                      for b in range(16)])).cuda()
+        o1 = cuda.full((16,), float("nan"), dtype=cuda.float64, device="cuda")
+        o2 = cuda.full((16,), float("nan"), dtype=cuda.float64, device="cuda")
+        spmiqc.check(f(n_small, 16, spmiqc.SPM_FP64, A.data_ptr(), B.data_ptr(), o1.data_ptr(), stream))
+        spmiqc.check(f(n_small, 16, spmiqc.SPM_FP64, B.data_ptr(), B.data_ptr(), o2.data_ptr(), stream))
+        a, bb = A.cpu().numpy(), B.cpu().numpy()
+        e1 = (a * bb).sum(1) / n_small
+        e2 = (bb * bb).sum(1) / n_small
+        assert np.allclose(o1.cpu().numpy(), e1, rtol=1e-12, atol=1e-300), n_small
+        assert np.allclose(o2.cpu().numpy(), e2, rtol=1e-12, atol=1e-300), n_small
     # above the stated maximum: refused on the host with SPM_ERR_ARG
     big = cuda.zeros((17, 2), dtype=cuda.float64, device="cuda")
     rc = f(2, 17, spmiqc.SPM_FP64, big.data_ptr(), big.data_ptr(), out.data_ptr(), stream)
