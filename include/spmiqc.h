@@ -86,15 +86,18 @@ const char *spm_status_str(int status);
  * 3 = direct loads, three CTAs per SM (fewer registers per thread), 4 = four
  * CTAs per SM for the exchanges through L2 of FP32 gradient chains (3
  * elsewhere), 5 = CTAs of 16 rows and 128 threads, four per SM, for gradient
- * chains with both exchanges through L2 (2 elsewhere).
+ * chains with both exchanges through L2 (2 elsewhere), 6 = as 5 with the
+ * fused plane pass software-pipelined over x-planes (each exchange's cluster
+ * barrier split into arrive and wait with a neighbouring plane's work in
+ * between; the same bits).
  * knob "fuse_planes": 1 (default) = chains of gradient steps join each step's
  * inverse plane pass with the next step's forward one (phi stays on chip
  * between steps; the same bits as 0), 0 = three passes per step.
- * knob "plane_xg" (0..3, plane_cps 2 to 5): the plane kernels of
+ * knob "plane_xg" (0..3, plane_cps 2 to 6): the plane kernels of
  * gradient chains exchange the x-plane between the CTAs of a cluster through
  * distributed shared memory (0) or through per-CTA areas in global memory that
  * stay resident in L2 (bit 1: the forward exchange, bit 2: the inverse one;
- * the same bits either way). Nonzero allocates the areas (2 x resident CTAs x
+ * the same bits either way). Nonzero allocates the areas (4 x resident CTAs x
  * 16 N complex values).
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
@@ -102,7 +105,7 @@ int spm_tune_get(const spm_ctx *ctx, const char *knob);
 /* Autotuner (no counterpart in the reference): times chains of `steps`
  * gradient steps on a scratch field for each candidate schedule (plane_cps
  * 1/2/3 with fused chains, plane_cps 2 without, plane_xg 1/2/3 with plane_cps
- * 2 and 3 on fused chains, plane_cps 4 for FP32, 5) and keeps the fastest in the
+ * 2 and 3 on fused chains, plane_cps 4 for FP32, 5, 6) and keeps the fastest in the
  * context; the choice is remembered per (device, N, precision), so later
  * contexts of the same kind take it without timing (FP32 twins of mixed flows
  * included). Synchronises; allocates two scratch fields while it runs. The

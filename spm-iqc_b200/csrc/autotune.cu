@@ -91,6 +91,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   std::vector<Choice> all(std::begin(cands), std::end(cands));
   if (c->prec == SPM_FP32) all.push_back({4, 1, spm::kXgFwd | spm::kXgInv});  // four CTAs per SM
   all.push_back({5, 1, spm::kXgFwd | spm::kXgInv});  // 16-row CTAs, four per SM
+  all.push_back({6, 1, spm::kXgFwd | spm::kXgInv});  // the same, fused pass pipelined over planes
   for (const Choice &cand : all) {
     if (rc != SPM_OK) break;
     c->plane_cps = cand.plane_cps;

@@ -32,6 +32,7 @@ constexpr int kCols = 16;       // y-lines (spectral columns) per CTA, plane ker
 // C2R rows) go through distributed shared memory, or, with these bits, through
 // per-CTA global areas that stay resident in L2.
 constexpr int kXgFwd = 1, kXgInv = 2;
+constexpr int kXgRegions = 4;   // exchange-area regions: two per exchange
 constexpr int kMaxBatch = 16;   // fields per launch
 constexpr int kScal = 16;       // scalars per field in the scalar block
 constexpr int kRedMax = 8;      // reduction slots per field and CTA
@@ -206,6 +207,25 @@ __device__ __forceinline__ void combine(double (&a)[NR], const double (&b)[NR]) 
   for (int r = 0; r < NR; r++) a[r] = ((MAXM >> r) & 1u) ? fmax(a[r], b[r]) : a[r] + b[r];
 }
 
+// FP32 partial sums of the FP32 kernels. A policy with FACC = true takes
+// its accumulator array as a template parameter; in FP32 kernels a thread then
+// sums the contributions of one batch of its points (16 to 32 values) in FP32
+// and folds that partial into its FP64 accumulator, in place of an FP32 ->
+// FP64 conversion and FP64 arithmetic per point (FP64 kernels accumulate in
+// FP64 as before).
+template <class X, class = void> struct HasFacc : std::false_type {};
+template <class X> struct HasFacc<X, std::void_t<decltype(X::FACC)>> : std::bool_constant<X::FACC> {};
+template <class T, class X> constexpr bool use_facc() { return sizeof(T) == 4 && HasFacc<X>::value; }
+
+template <int NR, unsigned MAXM> __device__ __forceinline__ void facc_init(float (&a)[NR]) {
+#pragma unroll
+  for (int r = 0; r < NR; r++) a[r] = ((MAXM >> r) & 1u) ? -3.0e38f : 0.0f;
+}
+template <int NR, unsigned MAXM> __device__ __forceinline__ void facc_fold(double (&acc)[NR], const float (&a)[NR]) {
+#pragma unroll
+  for (int r = 0; r < NR; r++) acc[r] = ((MAXM >> r) & 1u) ? fmax(acc[r], (double)a[r]) : acc[r] + (double)a[r];
+}
+
 // Deterministic block reduction (fixed butterfly + fixed warp order).
 // The result is valid in thread 0. scratch: 32 * NR doubles of shared memory.
 template <int NR, unsigned MAXM>
@@ -366,6 +386,10 @@ __device__ __forceinline__ void cluster_arrive_relaxed() {
   asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
+// Arrive with release semantics (the default of barrier.cluster.arrive): the
+// CTA's earlier writes are visible to every thread of the cluster after its
+// matching wait (acquire).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
   asm volatile(
@@ -446,8 +470,9 @@ struct KParams {
   double *stats;        // grad-flow per-step records (or null)
   const double4 *gtab;  // per K^2 = Kx^2+Ky^2+Kz^2: {G, 1/(1+dt G), 1/(G+|Tau|+0.02), 1/(1+G)}
   int *err;             // set when a bounded wait timed out
-  void *xg;             // plane kernels with XG: global exchange areas, 2 x xg_cap CTAs x PLANE_UNITS complex
+  void *xg;             // plane kernels with XG: global exchange areas, xg_regions x xg_cap CTAs x PLANE_UNITS complex
   int xg_cap;
+  int xg_regions;
   int nb;
 };
 

@@ -81,19 +81,20 @@ __device__ __forceinline__ bool flow_stopped(const KParams &p) {
   return p.flow != nullptr && *((volatile const int *)p.flow + FW_GO) == 0;
 }
 
-// This CTA's global exchange area (e = 0: inverse exchange, 1: forward) and
-// that of rank 0 of its cluster (the cluster's CTAs are consecutive in x).
-// Each of the two regions holds xg_cap areas of 16 N complex values (32-row
-// CTAs), or twice as many of 8 N (16-row CTAs).
-template <int N, class T, int RW = kRows> struct XgAreas {
-  c2<T> *own[2] = {nullptr, nullptr};
-  const c2<T> *first[2] = {nullptr, nullptr};
+// This CTA's global exchange area in region e (e = 0: inverse exchange, 1:
+// forward; the software-pipelined fused pass also uses 2 and 3, a second
+// area of each) and that of rank 0 of its cluster (the cluster's CTAs are
+// consecutive in x). Each region holds xg_cap areas of 16 N complex values
+// (32-row CTAs), or twice as many of 8 N (16-row CTAs).
+template <int N, class T, int RW = kRows, int R = 2> struct XgAreas {
+  c2<T> *own[R] = {};
+  const c2<T> *first[R] = {};
   __device__ XgAreas(const KParams &p, int rank) {
     if (p.xg == nullptr) return;
     constexpr size_t U = (size_t)RW * (N / 2);
     const size_t region = (size_t)p.xg_cap * Geo<N>::PLANE_UNITS;
     c2<T> *xg = reinterpret_cast<c2<T> *>(p.xg);
-    for (int e = 0; e < 2; e++) {
+    for (int e = 0; e < R; e++) {
       own[e] = xg + e * region + (size_t)blockIdx.x * U;
       first[e] = xg + e * region + (size_t)(blockIdx.x - rank) * U;
     }
@@ -146,7 +147,7 @@ template <int N, class T, int RW = kRows> struct Plane {
   // warp on its own rows. Ends with a cluster barrier: the rows [r][M] are
   // then ready for remote reads, in buf or (XG) in the CTA's global exchange
   // area gx.
-  template <bool XG = false>
+  template <bool XG = false, bool SYNC = true>
   __device__ static void zf2_post(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, T2 *gx = nullptr) {
     const int warp = tid >> 5, lane = tid & 31;
     {
@@ -204,7 +205,7 @@ template <int N, class T, int RW = kRows> struct Plane {
         }
       }
     }
-    cluster.sync();
+    if constexpr (SYNC) cluster.sync();
   }
 
   // forward y over this CTA's 16 columns: gather element y = 16*j1 + j2 of
@@ -270,7 +271,7 @@ template <int N, class T, int RW = kRows> struct Plane {
   // inverse y over this CTA's 16 columns; ld(ky, c) returns the input value.
   // Leaves y-line values at ycol(y, c) in buf (or, XG, in the CTA's global
   // exchange area gx) and ends with a cluster barrier.
-  template <bool XG = false, class LD>
+  template <bool XG = false, class LD, bool SYNC = true>
   __device__ static void yi(T2 *buf, const T2 *tw, int tid, cg::cluster_group &cluster, LD ld, T2 *gx = nullptr) {
     {
       const int c = tid % CW, j2 = tid / CW;
@@ -298,7 +299,7 @@ template <int N, class T, int RW = kRows> struct Plane {
         else buf[k1 * XS + k2 * CW + c] = u[k2];
       }
     }
-    cluster.sync();
+    if constexpr (SYNC) cluster.sync();
   }
 
   // Complex-to-real pre-processing fused with stage 1 of the inverse z
@@ -491,11 +492,21 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
       const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
       const T2 *row = STAGED ? stage + r * (N / 2) : reinterpret_cast<const T2 *>(src + rowoff);
       T2 v[N1];
-      sfor<0, N1>([&](auto J1) {
-        constexpr int j1 = SPM_CI(J1);
-        const int j = j1 * 8 + j2;
-        v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : ld_stream(row + j, spol), acc);
-      });
+      auto prologue = [&](auto &a) {
+        sfor<0, N1>([&](auto J1) {
+          constexpr int j1 = SPM_CI(J1);
+          const int j = j1 * 8 + j2;
+          v[j1] = Pro::pro(p, b, rowoff + 2 * j, STAGED ? row[j] : ld_stream(row + j, spol), a);
+        });
+      };
+      if constexpr (use_facc<T, Pro>()) {
+        float fa[Pro::NR];
+        facc_init<Pro::NR, Pro::MAXM>(fa);
+        prologue(fa);
+        facc_fold<Pro::NR, Pro::MAXM>(acc, fa);
+      } else {
+        prologue(acc);
+      }
       P::zf1_store(buf, ztw, v, r, j2);
     }
     if (STAGED) __syncthreads();  // every row of the stage is read
@@ -688,7 +699,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
       }
     }
     // the per-point operator
-    if (has2) {
+    auto point_ops = [&](auto &acc) {
       T2 *so = Op::SO ? reinterpret_cast<T2 *>(p.sto[b]) : nullptr;
       const int Ky = wave(ky, N);
       const int pr = (t == 0) ? rowsel : 1 - rowsel;
@@ -723,6 +734,16 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
         }
         if constexpr (Op::SO) st_stream(so + ((size_t)kx * N + ky) * M + col, o_st, spol);
         F[k2] = o_inv;
+      }
+    };
+    if (has2) {
+      if constexpr (use_facc<T, Op>()) {
+        float fa[Op::NR];
+        facc_init<Op::NR, Op::MAXM>(fa);
+        point_ops(fa);
+        facc_fold<Op::NR, Op::MAXM>(acc, fa);
+      } else {
+        point_ops(acc);
       }
     }
     __syncthreads();  // sS, stab and ex reads done
@@ -927,11 +948,21 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_kernel(const __grid
         const int j2 = tid & 7, r = tid >> 3;
         const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
         T2 v[N1];
-        sfor<0, N1>([&](auto J1) {
-          constexpr int j1 = SPM_CI(J1);
-          const int j = j1 * 8 + j2;
-          v[j1] = Pro::pro(p, b, rowoff + 2 * j, buf[r * M + j], acc_p);
-        });
+        auto prologue = [&](auto &a) {
+          sfor<0, N1>([&](auto J1) {
+            constexpr int j1 = SPM_CI(J1);
+            const int j = j1 * 8 + j2;
+            v[j1] = Pro::pro(p, b, rowoff + 2 * j, buf[r * M + j], a);
+          });
+        };
+        if constexpr (use_facc<T, Pro>()) {
+          float fa[Pro::NR];
+          facc_init<Pro::NR, Pro::MAXM>(fa);
+          prologue(fa);
+          facc_fold<Pro::NR, Pro::MAXM>(acc_p, fa);
+        } else {
+          prologue(acc_p);
+        }
         __syncwarp();  // the warp's rows are read before its z exchange overwrites them
         P::zf1_store(buf, ztw, v, r, j2);
       }
@@ -941,6 +972,165 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_kernel(const __grid
     }
     __syncthreads();
   }
+  double all[NA], tot[NA];
+#pragma unroll
+  for (int r = 0; r < NE; r++) all[r] = acc_e[r];
+#pragma unroll
+  for (int r = 0; r < NP; r++) all[NE + r] = acc_p[r];
+  if constexpr (NE + NP == 0) all[0] = 0.0;
+  if (grid_reduce<NA, (Epi::MAXM | (Pro::MAXM << NE))>(all, red, p.partials + (size_t)b * kPartStride * kRedMax,
+                                                        p.tickets + b, gridDim.x, blockIdx.x, tot)) {
+    double te[NE > 0 ? NE : 1], tp[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int r = 0; r < NE; r++) te[r] = tot[r];
+#pragma unroll
+    for (int r = 0; r < NP; r++) tp[r] = tot[NE + r];
+    Epi::fin(p, b, te);
+    if (!stop) Pro::fin(p, b, tp);
+  }
+}
+
+
+// --------------------------------------------------------------- plane_inv_fwd, pipelined
+// plane_inv_fwd with both exchanges through the L2 areas, software-pipelined
+// over the cluster's x-planes. A plane is three phases:
+//   A(p): inverse y of this CTA's columns (loads B), into its inverse area;
+//   Z(p): C2R z from every CTA's inverse area, epilogue, prologue, R2C z,
+//         into its forward area;
+//   Y(p): forward y from every CTA's forward area, stores A.
+// Each exchange needs a cluster barrier between the writes of one phase and
+// the reads of the next. Here the barrier is split into its arrive (release)
+// and its wait (acquire), with independent work of a neighbouring plane in
+// between, so the CTA computes while the slowest CTA of its cluster catches up:
+//   step i = 0 .. n: A(p_i), Y(p_i-1), Z(p_i) (the phases that exist)
+// with the forward barrier of p_i-1 spanning A(p_i) and the inverse barrier of
+// p_i spanning Y(p_i-1). Planes alternate between two inverse and two forward
+// areas (regions 0/2 and 1/3): an area is rewritten two planes later, after a
+// barrier every reader passed after its last read. The arithmetic is that of
+// plane_inv_fwd, so results are identical. The stopping step (FW_PENDING)
+// runs the inverse half only, as plane_inv_fwd does.
+template <int N, class T, class Epi, class Pro, int CPS, int RW>
+__global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_pipe_kernel(const __grid_constant__ KParams p) {
+  using G = Geo<N>;
+  using T2 = c2<T>;
+  using P = Plane<N, T, RW>;
+  constexpr int M = G::M, N1 = G::N1;
+  constexpr int NE = Epi::NR, NP = Pro::NR, NA = (NE + NP > 0) ? NE + NP : 1;
+  static_assert(NA <= kRedMax, "reduction count");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
+  T2 *ztw = tw + N;
+  T2 *buf = ztw + N / 2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
+  double *red = reinterpret_cast<double *>(bar + 2);
+  if (flow_stopped(p)) return;
+  const bool stop = p.flow != nullptr && *((volatile const int *)p.flow + FW_PENDING) != 0;
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int tid = threadIdx.x;
+  const int b = blockIdx.y;
+  const int rank = (int)cluster.block_rank();
+  const XgAreas<N, T, RW, 4> xa(p, rank);
+  const uint64_t spol = l2_stream_policy();
+  const int cid = blockIdx.x / P::CL, ncl = gridDim.x / P::CL;
+  plane_twiddles<N, T>(p, tw, ztw);
+  double acc_e[NE > 0 ? NE : 1], acc_p[NP > 0 ? NP : 1];
+#pragma unroll
+  for (int r = 0; r < (NE > 0 ? NE : 1); r++) acc_e[r] = ((Epi::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+#pragma unroll
+  for (int r = 0; r < (NP > 0 ? NP : 1); r++) acc_p[r] = ((Pro::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
+  __syncthreads();
+  const T2 *gsrc = reinterpret_cast<const T2 *>(p.in[b]);
+  T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
+  T *phi = reinterpret_cast<T *>(p.sto[b]);
+
+  // A(plane) into inverse area `slot` (no barrier)
+  auto phase_a = [&](int plane, int slot) {
+    if (plane + ncl < N)
+      for (int i = tid; i < N; i += P::TH)
+        prefetch_l2(gsrc + ((size_t)(plane + ncl) * N + i) * M + rank * P::CW, P::CW * sizeof(T2));
+    auto ld = [&](int ky, int c) -> T2 {
+      return ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * P::CW + c, spol);
+    };
+    P::template yi<true, decltype(ld), false>(buf, tw, tid, cluster, ld, slot ? xa.own[2] : xa.own[0]);
+  };
+  // Z(plane) from the inverse areas `slot` into forward area `slot` (no barrier)
+  auto phase_z = [&](int plane, int slot) {
+    P::template c2r_zi1<true>(buf, tw, ztw, tid, rank, cluster, slot ? xa.first[2] : xa.first[0]);
+    P::template zi2<true>(buf, tid, [&](int r, int j, T2 z) {
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
+      buf[r * M + j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
+    });
+    __syncwarp();
+    {
+      const int j2 = tid & 7, r = tid >> 3;
+      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
+      T2 v[N1];
+      auto prologue = [&](auto &a) {
+        sfor<0, N1>([&](auto J1) {
+          constexpr int j1 = SPM_CI(J1);
+          const int j = j1 * 8 + j2;
+          v[j1] = Pro::pro(p, b, rowoff + 2 * j, buf[r * M + j], a);
+        });
+      };
+      if constexpr (use_facc<T, Pro>()) {
+        float fa[Pro::NR];
+        facc_init<Pro::NR, Pro::MAXM>(fa);
+        prologue(fa);
+        facc_fold<Pro::NR, Pro::MAXM>(acc_p, fa);
+      } else {
+        prologue(acc_p);
+      }
+      __syncwarp();
+      P::zf1_store(buf, ztw, v, r, j2);
+    }
+    __syncwarp();
+    P::template zf2_post<true, false>(buf, tw, tid, cluster, slot ? xa.own[3] : xa.own[1]);
+  };
+  // Y(plane) from the forward areas `slot`, stores A
+  auto phase_y = [&](int plane, int slot) {
+    P::template yf<true>(buf, tw, tid, rank, cluster, dst, plane, slot ? xa.first[3] : xa.first[1]);
+  };
+
+  if (stop) {
+    for (int plane = cid; plane < N; plane += ncl) {
+      P::template yi<true>(
+          buf, tw, tid, cluster,
+          [&](int ky, int c) -> T2 { return ld_stream(gsrc + ((size_t)plane * N + ky) * M + rank * P::CW + c, spol); },
+          xa.own[0]);
+      P::template c2r_zi1<true>(buf, tw, ztw, tid, rank, cluster, xa.first[0]);
+      P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
+        reinterpret_cast<T2 *>(phi + rowoff)[j] = Epi::epi(p, b, rowoff + 2 * j, z, acc_e);
+      });
+      // keeps the inverse areas of this plane from being rewritten while a peer still reads them
+      cluster.sync();
+    }
+  } else {
+    // planes cid + i * ncl, i < n (the same n on every CTA of the cluster);
+    // step i runs A(p_i), Y(p_i-1), Z(p_i), each phase written once
+    const int n = cid < N ? (N - cid + ncl - 1) / ncl : 0;
+    for (int i = 0; i <= n; i++) {
+      const int plane = cid + i * ncl;
+      if (i < n) {
+        __syncthreads();
+        phase_a(plane, i & 1);
+      }
+      if (i > 0) cluster_wait();    // forward areas of p_i-1 complete
+      if (i < n) cluster_arrive();  // inverse areas of p_i written
+      if (i > 0) {
+        __syncthreads();
+        phase_y(plane - ncl, (i - 1) & 1);
+      }
+      if (i < n) {
+        cluster_wait();  // inverse areas of p_i complete
+        __syncthreads();
+        phase_z(plane, i & 1);
+        cluster_arrive();  // forward areas of p_i written
+      }
+    }
+  }
+  __syncthreads();
   double all[NA], tot[NA];
 #pragma unroll
   for (int r = 0; r < NE; r++) all[r] = acc_e[r];

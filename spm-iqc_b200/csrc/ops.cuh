@@ -33,13 +33,16 @@ template <class T> __device__ __forceinline__ T poly_energy(T u, T mtau2, T mgam
 }
 
 // Gradient step (LPsrc.cpp:44-75): transform f(u) and sum the energy density.
+// FACC: in FP32 the energy density is summed in FP32 over a row's points of
+// one thread before it joins the FP64 total.
 template <class T> struct ProGrad {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
-  __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, double (&acc)[1]) {
+  static constexpr bool FACC = true;
+  template <class A> __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, A (&acc)[1]) {
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
     const T mtau2 = (T)(-0.5 * p.m.Tau), mgam3 = (T)(-p.m.Gamma / 3.0);
-    acc[0] += (double)poly_energy(x.x, mtau2, mgam3) + (double)poly_energy(x.y, mtau2, mgam3);
+    acc[0] += (A)poly_energy(x.x, mtau2, mgam3) + (A)poly_energy(x.y, mtau2, mgam3);
     return c2<T>{poly_force(x.x, tau, gam), poly_force(x.y, tau, gam)};
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
@@ -185,25 +188,31 @@ template <class T> struct OpInv {
 // ||grad F|| of the incoming state:
 //   u' = (dt f^ + u) / (1 + dt G), u'_0 = 0,  res = max |Re(u' - u)|,
 //   E1 = 1/2 sum G |u|^2,  ||grad F||^2 = sum_{k != 0} |G u - f^|^2.
+// FACC: in FP32 the three reductions run in FP32 over a thread's 16 points of
+// a tile (the differences G u - f^ and u' - u of FP32 values, which carry
+// FP32 rounding already), then join the FP64 totals.
 template <class T> struct OpGrad {
   static constexpr bool FI = true, SI = true, SO = true, INV = true, LIN = false;
   static constexpr int SYM = 0;  // {G, 1/(1 + dt G)}
   static constexpr int NR = 3;
   static constexpr unsigned MAXM = 0x2;
+  static constexpr bool FACC = true;
+  template <class A>
   __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T> s, c2<T> &so,
-                               c2<T> &inv, double (&acc)[3], double w) {
-    const double G = sy.x;
+                               c2<T> &inv, A (&acc)[3], double w) {
+    const A G = (A)sy.x;
     const T dt = (T)p.m.dt;
     const c2<T> fh = cscale(f, (T)p.m.inv_n3);
     const T iden = (T)sy.y;  // 1 / (1 + dt G)
     c2<T> u1 = {(dt * fh.x + s.x) * iden, (dt * fh.y + s.y) * iden};
     const bool k0 = (Kx == 0 && Ky == 0 && Kz == 0);
     if (k0) u1 = c2<T>{0, 0};
-    acc[0] += w * 0.5 * G * ((double)s.x * (double)s.x + (double)s.y * (double)s.y);
-    acc[1] = fmax(acc[1], fabs((double)u1.x - (double)s.x));
+    const A wa = (A)w;
+    acc[0] += wa * (A)0.5 * G * ((A)s.x * (A)s.x + (A)s.y * (A)s.y);
+    acc[1] = fmax(acc[1], fabs((A)u1.x - (A)s.x));
     if (!k0) {
-      const double gx = G * (double)s.x - (double)fh.x, gy = G * (double)s.y - (double)fh.y;
-      acc[2] += w * (gx * gx + gy * gy);
+      const A gx = G * (A)s.x - (A)fh.x, gy = G * (A)s.y - (A)fh.y;
+      acc[2] += wa * (gx * gx + gy * gy);
     }
     so = u1;
     inv = u1;

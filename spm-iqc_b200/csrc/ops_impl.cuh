@@ -35,7 +35,7 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
 // (queried once per kernel and device), at most one per x-plane.
 template <class Tag, int N, class K, int RW = kRows>
 static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int nb, const char *what,
-                          bool xg = false) {
+                          bool xg = false, int regions = 2) {
   constexpr int CLr = N / RW;
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
   if (e == cudaSuccess && CLr > 8) {  // clusters of up to 16 CTAs (16-row CTAs at N = 256)
@@ -73,7 +73,7 @@ static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int
   }
   cfg.gridDim = dim3(CLr * nc, nb, 1);
   // a kernel exchanging through global areas needs one per CTA (nb == 1)
-  if (xg && (!p.xg || nb != 1 || CLr * nc > p.xg_cap * (kRows / RW)))
+  if (xg && (!p.xg || nb != 1 || CLr * nc > p.xg_cap * (kRows / RW) || p.xg_regions < regions))
     return spm_fail(SPM_ERR_STATE, "plane exchange areas missing or too small");
   c->launches++;
   e = cudaLaunchKernelEx(&cfg, kern, p);
@@ -88,9 +88,11 @@ template <class T> struct XgOk<ProGrad<T>> : std::true_type {};
 template <class T> struct XgOk<EpiFlow<T>> : std::true_type {};
 // plane_cps 5: gradient chains with both exchanges through L2 run 16-row CTAs
 // (128 threads, four per SM, 128 registers each); other chains run as with 2.
-static inline int eff_cps(const spm_ctx *c) { return c->plane_cps == 5 ? 2 : c->plane_cps; }
+// plane_cps 6: the same, with the fused pass software-pipelined over planes.
+static inline bool cps_rw16(const spm_ctx *c) { return c->plane_cps == 5 || c->plane_cps == 6; }
+static inline int eff_cps(const spm_ctx *c) { return cps_rw16(c) ? 2 : c->plane_cps; }
 static inline int xg_bits(const spm_ctx *c, int nb) { return (c->xg && nb == 1 && eff_cps(c) >= 2) ? c->plane_xg : 0; }
-static inline bool rw16(const spm_ctx *c, int nb) { return c->plane_cps == 5 && xg_bits(c, nb) == (kXgFwd | kXgInv); }
+static inline bool rw16(const spm_ctx *c, int nb) { return cps_rw16(c) && xg_bits(c, nb) == (kXgFwd | kXgInv); }
 // Four CTAs per SM (64 registers per thread): FP32 gradient chains only.
 template <class T> static inline bool cps4(const spm_ctx *c) { return sizeof(T) == 4 && eff_cps(c) == 4; }
 
@@ -194,8 +196,14 @@ static int plane_inv_fwd_xg(spm_ctx *c, const KParams &p, int nb) {
 template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx *c, const KParams &p, int nb) {
   if constexpr (XgOk<Pro>::value && XgOk<Epi>::value) {
     if (rw16(c, nb)) {
-      struct Tag16 {};
       constexpr int XG = kXgFwd | kXgInv;
+      if (c->plane_cps == 6) {
+        struct Tag16p {};
+        return launch_cluster<Tag16p, N, decltype(&plane_inv_fwd_pipe_kernel<N, T, Epi, Pro, 4, 16>), 16>(
+            c, plane_inv_fwd_pipe_kernel<N, T, Epi, Pro, 4, 16>, plane_smem<N, T, 4, 16>(), p, nb,
+            "plane_inv_fwd (pipelined)", true, 4);
+      }
+      struct Tag16 {};
       return launch_cluster<Tag16, N, decltype(&plane_inv_fwd_kernel<N, T, Epi, Pro, 4, XG, 16>), 16>(
           c, plane_inv_fwd_kernel<N, T, Epi, Pro, 4, XG, 16>, plane_smem<N, T, 4, 16>(), p, nb, "plane_inv_fwd", true);
     }

@@ -86,10 +86,12 @@ KParams spm_params(const spm_ctx *c) {
   p.err = c->flow + FW_ERR;
   p.xg = c->xg;
   p.xg_cap = c->xg_cap;
+  p.xg_regions = c->xg ? spm::kXgRegions : 0;
   return p;
 }
 
-// One area per resident CTA of a plane kernel and exchange: at most
+// One area per resident CTA of a plane kernel, exchange and region (two
+// regions per exchange, for the software-pipelined fused pass): at most
 // min(SMs x CTAs per SM, N x CL) CTAs, the CTAs per SM bounded by the plane
 // kernels' shared memory and 8 blocks of 256 threads.
 int spm_ensure_xg(spm_ctx *c) {
@@ -105,7 +107,7 @@ int spm_ensure_xg(spm_ctx *c) {
   per_sm = per_sm < 1 ? 1 : (per_sm > 8 ? 8 : per_sm);
   const int most = c->N * (c->N / spm::kRows);
   const int cap = sms * per_sm < most ? sms * per_sm : most;
-  e = cudaMalloc(&c->xg, 2 * (size_t)cap * units * cplx);
+  e = cudaMalloc(&c->xg, (size_t)spm::kXgRegions * cap * units * cplx);
   if (e != cudaSuccess) {
     c->xg = nullptr;
     return spm_fail_cuda(e, "plane exchange areas");
@@ -363,7 +365,7 @@ extern "C" int spm_ctx_destroy(spm_ctx *c) {
 extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
   if (!c || !knob) return spm_fail(SPM_ERR_ARG, "null argument");
   if (std::strcmp(knob, "plane_cps") == 0) {
-    if (value < 1 || value > 5) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1 to 5");
+    if (value < 1 || value > 6) return spm_fail(SPM_ERR_ARG, "plane_cps must be 1 to 6");
     c->plane_cps = value;
     return SPM_OK;
   }

@@ -137,12 +137,13 @@ def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
 @pytest.mark.parametrize("N,prec", [(64, "fp64"), (96, "fp64"), (256, "fp64"), (128, "fp32"), (192, "fp32")])
 def test_exchange_routes_are_bit_identical(spm, cuda, N, prec):
     """Gradient chains whose plane kernels exchange through global areas in L2
-    (plane_xg 1, 2, 3; plane_cps 2, 3, 5 (16-row CTAs) and, in FP32, 4) give the same fields as exchanges
+    (plane_xg 1, 2, 3; plane_cps 2, 3, 5 (16-row CTAs), 6 (the same, pipelined over planes) and, in
+    FP32, 4) give the same fields as exchanges
     through distributed shared memory, and records equal to rounding."""
     phi = npo.uniform_field(N, 12)
     dt = np.float64 if prec == "fp64" else np.float32
     out = []
-    combos = ((2, 0), (2, 1), (2, 2), (2, 3), (3, 3), (5, 3)) + (((4, 3), (4, 0)) if prec == "fp32" else ())
+    combos = ((2, 0), (2, 1), (2, 2), (2, 3), (3, 3), (5, 3), (6, 3)) + (((4, 3), (4, 0)) if prec == "fp32" else ())
     for cps, xg in combos:
         e = spm.SpmContext(N, Tau=-0.02, precision=prec)
         e.tune("plane_cps", cps)
