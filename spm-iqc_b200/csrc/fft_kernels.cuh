@@ -857,11 +857,21 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_kernel(const __grid_con
       issue(next);
     }
     P::template c2r_zi1<(XG & kXgInv) != 0>(buf, tw, ztw, tid, rank, cluster, xa.first[it & 1]);
-    P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
-      const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
-      const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, acc);
-      if (outb) reinterpret_cast<T2 *>(outb + rowoff)[j] = val;
-    });
+    auto epilogue = [&](auto &a) {
+      P::template zi2<false>(buf, tid, [&](int r, int j, T2 z) {
+        const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
+        const T2 val = Epi::epi(p, b, rowoff + 2 * j, z, a);
+        if (outb) reinterpret_cast<T2 *>(outb + rowoff)[j] = val;
+      });
+    };
+    if constexpr (use_facc<T, Epi>()) {
+      float fa[Epi::NR];
+      facc_init<Epi::NR, Epi::MAXM>(fa);
+      epilogue(fa);
+      facc_fold<Epi::NR, Epi::MAXM>(acc, fa);
+    } else {
+      epilogue(acc);
+    }
     __syncthreads();
   }
   report_error(p, s_err);

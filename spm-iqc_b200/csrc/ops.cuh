@@ -105,19 +105,22 @@ template <class T> struct ProPrecond {
 //   <f, v> = -<x, Gv> + <N, v> - mean(N) mean(v),  f = ngrad(x),
 // where Gv = IFFT(G FFT(v), k = 0 removed) is prepared once per tangent.
 // aux0 = v, aux1 = Gv.
+// FACC: in FP32 the four sums run in FP32 over a row's points of one thread
+// before they join the FP64 totals.
 template <class T> struct ProForce {
   static constexpr int NR = 4;
   static constexpr unsigned MAXM = 0;
-  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[4]) {
+  static constexpr bool FACC = true;
+  template <class A> __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, A (&acc)[4]) {
     const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
     const c2<T> gv = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
     const T n0 = poly_force(x.x, tau, gam);
     const T n1 = poly_force(x.y, tau, gam);
-    acc[0] += (double)x.x * (double)gv.x + (double)x.y * (double)gv.y;
-    acc[1] += (double)n0 * (double)v.x + (double)n1 * (double)v.y;
-    acc[2] += (double)n0 + (double)n1;
-    acc[3] += (double)v.x + (double)v.y;
+    acc[0] += (A)x.x * (A)gv.x + (A)x.y * (A)gv.y;
+    acc[1] += (A)n0 * (A)v.x + (A)n1 * (A)v.y;
+    acc[2] += (A)n0 + (A)n1;
+    acc[3] += (A)v.x + (A)v.y;
     return c2<T>{x.x + n0, x.y + n1};
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[4]) {
@@ -132,10 +135,11 @@ template <class T> struct ProForce {
 template <class T> struct ProTangent {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
-  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[1]) {
+  static constexpr bool FACC = true;
+  template <class A> __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, A (&acc)[1]) {
     const c2<T> a = p.aux0[b] ? __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx)) : c2<T>{0, 0};
     const c2<T> d = {x.x - a.x, x.y - a.y};
-    acc[0] += (double)d.x * (double)d.x + (double)d.y * (double)d.y;
+    acc[0] += (A)d.x * (A)d.x + (A)d.y * (A)d.y;
     return d;
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
@@ -368,14 +372,15 @@ template <class T> struct EpiFlow {
 template <class T> struct EpiNgrad {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
-  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&acc)[1]) {
+  static constexpr bool FACC = true;
+  template <class A> __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, A (&acc)[1]) {
     const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
     const T mg = -(T)scal_of(p, b)[SC_MU];
     c2<T> o;
     o.x = -((y.x - tau * ph.x - gam * (ph.x * ph.x) + ph.x * ph.x * ph.x) - mg);
     o.y = -((y.y - tau * ph.y - gam * (ph.y * ph.y) + ph.y * ph.y * ph.y) - mg);
-    acc[0] += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+    acc[0] += (A)o.x * (A)o.x + (A)o.y * (A)o.y;
     return o;
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
