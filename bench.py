@@ -371,16 +371,20 @@ def batch_bench(args):
     fields = [workloads.field(s, device="cuda") for s in specs]
     cap, tol = args.batch_steps, 1e-8
     out = {}
-    for name in ("batched_mixed", "serial_fp64"):
+    arms = ("batched_mixed", "batched_mixed_branches", "serial_fp64") if args.batch_branches else \
+        ("batched_mixed", "serial_fp64")
+    for name in arms:
         ctxs = [spmiqc.SpmContext(s.N, L=s.L, Tau=s.Tau) for s in specs]
         for c, s in zip(ctxs, specs):
             c.autotune(20)
+            # batched_mixed: instances of one size share every launch; _branches: one branch per instance
+            c.tune("batch_group", 0 if name == "batched_mixed_branches" else 1)
         phis = [torch.from_numpy(f.copy()).cuda() for f in fields]
         uhs = [c.my_fft(p) for c, p in zip(ctxs, phis)]
         torch.cuda.synchronize()
         barrier(world)
         t0 = time.perf_counter()
-        if name == "batched_mixed":
+        if name.startswith("batched_mixed"):
             steps = spmiqc.batch_grad_flow(ctxs, phis, uhs, cap, tol, switch_tol=1e-7, steps_per_launch=32)
         else:
             steps = [len(c.get_min_u_F(p, u, cap, tol_grad=tol)) for c, p, u in zip(ctxs, phis, uhs)]
@@ -410,6 +414,9 @@ def batch_bench(args):
             "scaling": "weak", "speedup_vs_serial_fp64": b["seconds"] / a["seconds"],
             "batched_mixed": {k: a[k] for k in ("seconds", "instances_per_s", "steps", "reached_tol")},
             "serial_fp64": {k: b[k] for k in ("seconds", "instances_per_s", "steps", "reached_tol")},
+            "batched_mixed_branches": ({k: out["batched_mixed_branches"][k] for k in
+                                        ("seconds", "instances_per_s", "steps", "reached_tol")}
+                                       if "batched_mixed_branches" in out else None),
             "max_abs_energy_diff_where_both_converged": eabs, "max_rel_energy_diff_where_both_converged": ediff,
             "energy_range": [min(b["energy"]), max(b["energy"])], "data": "synthetic", "dtype": "f32+f64",
             "config": {"workload": "batched relaxations", "instances": [[s.N, round(s.L, 3), round(s.Tau, 5), s.shell]
@@ -459,6 +466,98 @@ def serve_bench(args):
                        "rate_per_s": 4.0 * world, "parallelism": f"jobs partitioned by footprint over {world} GPU(s)"}}
     print(json.dumps(line))
     return 0
+
+
+def config_legs(ctx, phi_h):
+    """The two 256^3 FP64 workloads beyond the timed flow (their own keys on the
+    benchmark line), from the same icosahedral phi0:
+
+    config2: semi-implicit gradient flow (LPsrc.cpp:40-117) to ||grad F|| <= 1e-8
+      in FP64 and in FP32 + FP64 polish, then LOBPCG k = 8 (LOBPCG.cpp:207-487)
+      to a residual <= 1e-8 at the end state. The stationary point this field
+      relaxes to has one negative Hessian eigenvalue and three near-zero
+      (translation) ones, so ||grad F|| bottoms out just above 1e-8: the flows
+      run to a step cap with tol 1e-8 (floor reported), and the FP64 / mixed
+      time comparison is made at tol_reached, the lowest tolerance both reach.
+    config3: Spring_Pairing (SPM.cpp:170-263) from that stationary point +- delta v1
+      (v1 the unstable eigenmode, nrmp(v1) = 1; delta = 0.001, the reference's
+      own separation, main_SPM.cpp:109-119) in FP64 and in FP32 + FP64 polish,
+      with the saddle energy and the unstable eigenvalue (LOBPCG k = 2 at the
+      saddle) of the mixed run against the all-FP64 run."""
+    import numpy as np
+    import torch
+    out = {"config2": {}, "config3": {}}
+    c2 = out["config2"]
+    tol, tol_r, cap, sw = 1e-8, 1.2e-8, 40000, 2e-8
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    runs = {}
+    for mode in ("fp64", "mixed"):
+        a = torch.from_numpy(phi_h.copy()).cuda()
+        ua = ctx.my_fft(a)
+        if mode == "fp64":
+            st, sec = timed(lambda: ctx.get_min_u_F(a, ua, cap, tol_grad=tol_r))
+            n32, n64 = 0, len(st)
+        else:
+            (st, n32, n64), sec = timed(lambda: ctx.get_min_u_F_mixed(a, ua, cap, tol_grad=tol_r, switch_tol=sw))
+        runs[mode] = (a, ua)
+        c2[mode] = {"tol": tol_r, "seconds": sec, "fp32_steps": n32, "fp64_steps": n64,
+                    "grad_norm": float(st[-1, 2]), "reached": bool(st[-1, 2] <= tol_r),
+                    "energy": ctx.get_Ene(a, ua)}
+    c2["mixed"]["switch_tol"] = sw
+    c2["speedup_mixed_vs_fp64"] = c2["fp64"]["seconds"] / c2["mixed"]["seconds"]
+    c2["energy_rel_diff_mixed_vs_fp64"] = abs(c2["mixed"]["energy"] - c2["fp64"]["energy"]) / abs(c2["fp64"]["energy"])
+    # the FP64 state continues toward 1e-8: where ||grad F|| bottoms out
+    a, ua = runs["fp64"]
+    del runs["mixed"]
+    st = ctx.get_min_u_F(a, ua, cap - c2["fp64"]["fp64_steps"], tol_grad=tol)
+    c2["toward_1e-8"] = {"tol": tol, "steps_total": c2["fp64"]["fp64_steps"] + len(st),
+                         "min_grad_norm": float(st[:, 2].min()), "reached": bool(st[:, 2].min() <= tol),
+                         "energy": ctx.get_Ene(a, ua)}
+    V = ctx.hiosd_lobpcg_initialization(8, seed=3)
+    (ev, rs, its), sec = timed(lambda: ctx.hiosd_lobpcg_inip(a, V, maxiter=800, tol=1e-8))
+    c2["lobpcg_k8"] = {"tol": 1e-8, "iterations": its, "seconds": sec, "iterations_per_s": its / sec,
+                       "evals": [float(x) for x in ev], "max_residual": float(max(rs)),
+                       "reached": bool(max(rs) <= 1e-8)}
+    v1 = V[0].clone()
+    del V
+    torch.cuda.empty_cache()
+    c3 = out["config3"]
+    delta, tol3, cap3, sw3 = 0.001, 1.1e-8, 3000, 3e-8
+    c3.update({"delta": delta, "tol": tol3, "cap": cap3})
+    for mode in ("fp64", "mixed"):
+        p0 = (a - delta * v1).contiguous()
+        p1 = (a + delta * v1).contiguous()
+        if mode == "fp64":
+            h, sec = timed(lambda: ctx.Spring_Pairing(p0, p1, cap3, tol3))
+            n32, n64 = 0, len(h)
+        else:
+            (h, n32, n64), sec = timed(lambda: ctx.Spring_Pairing_mixed(p0, p1, cap3, tol3, switch_tol=sw3))
+        mid = (0.5 * (p0 + p1)).contiguous()
+        um = ctx.my_fft(mid)
+        W = ctx.hiosd_lobpcg_initialization(2, seed=9)
+        ev, rs, lits = ctx.hiosd_lobpcg_inip(mid, W, maxiter=800, tol=1e-8)
+        c3[mode] = {"seconds": sec, "fp32_iterations": n32, "fp64_iterations": n64, "residual": float(h[-1]),
+                    "reached": bool(h[-1] <= tol3), "saddle_energy": ctx.get_Ene(mid, um),
+                    "unstable_eigenvalue": float(ev[0]), "lobpcg_iterations": lits,
+                    "lobpcg_residual": float(max(rs))}
+        del p0, p1, mid, um, W
+        torch.cuda.empty_cache()
+    c3["mixed"]["switch_tol"] = sw3
+    c3["speedup_mixed_vs_fp64"] = c3["fp64"]["seconds"] / c3["mixed"]["seconds"]
+    c3["saddle_energy_rel_err"] = abs(c3["mixed"]["saddle_energy"] - c3["fp64"]["saddle_energy"]) / abs(
+        c3["fp64"]["saddle_energy"])
+    c3["unstable_eigenvalue_rel_err"] = abs(c3["mixed"]["unstable_eigenvalue"] - c3["fp64"]["unstable_eigenvalue"]) / abs(
+        c3["fp64"]["unstable_eigenvalue"])
+    del a, ua, v1
+    torch.cuda.empty_cache()
+    return out
 
 
 def solver_legs(ctx, phi):
@@ -548,6 +647,7 @@ def main():
     ap.add_argument("--only-flow", action="store_true",
                     help="run only the warm-up and timed gradient steps (used for ncu captures)")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs mixed time-to-tolerance leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the config2 / config3 legs")
     ap.add_argument("--schedule", default=None,
                     help="plane_cps,fuse_planes,plane_xg for the FP64 context instead of the autotuner's choice "
                          "(fixed kernel variants for ncu captures)")
@@ -558,6 +658,8 @@ def main():
     ap.add_argument("--batch-n", type=int, default=24)
     ap.add_argument("--solvers", action="store_true", help="run only the LOBPCG and SPM legs (one JSON line)")
     ap.add_argument("--batch-steps", type=int, default=4000)
+    ap.add_argument("--batch-branches", action="store_true",
+                    help="--batch: also time the instances on separate branches (no shared launches)")
     ap.add_argument("--solvers-n", type=int, default=N, help="grid size of --solvers (small cases for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -741,6 +843,13 @@ def main():
         }
         del runs
 
+    configs = None
+    if world == 1 and not args.no_configs:
+        try:
+            configs = config_legs(ctx, phi_h)
+        except Exception as ex:  # reported, not fatal
+            configs = {"error": str(ex)[:300]}
+
     # end to end through the C ABI with the field in pinned host memory: per
     # step, upload phi, transform, one step, download phi and the step record
     ph_host = torch.from_numpy(phi_h.copy()).pin_memory()
@@ -798,7 +907,11 @@ def main():
             "cpu_baseline_serial": cpu_serial,
             "cpu_baseline_mkl": cpu_mkl,
             "parity": parity,
+            "config2": configs.get("config2") if configs else None,
+            "config3": configs.get("config3") if configs else None,
         }
+        if configs and "error" in configs:
+            line["configs_error"] = configs["error"]
         print(json.dumps(line))
     ctx.close()
     if world > 1:

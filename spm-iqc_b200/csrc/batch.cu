@@ -1,7 +1,12 @@
 // Batched gradient flows of independent instances (grids of any supported
 // sizes and parameters): one CUDA graph holds `steps_per_launch` gated steps of
-// every instance, each instance on its own stream branch, so one graph launch
-// advances all of them and small grids overlap on the device. Instances stop
+// every instance, so one graph launch advances all of them. Instances of the
+// same grid size and precision form groups of up to 16 that share every
+// launch (one launch per pass for the whole group, blockIdx.y = instance,
+// each instance with its own model, symbols and flow words); each group runs
+// on its own stream branch, so groups of different sizes overlap on the
+// device. (With the context knob "batch_group" = 0 on the first instance,
+// every instance gets its own branch and launches instead.) Instances stop
 // on the device (convergence or their step cap); the graph is relaunched until
 // every instance has stopped. With switch_tol > 0 the instances first run on
 // their FP32 twins (FP32 transforms, FP64 reductions) to switch_tol, then on
@@ -36,6 +41,37 @@ struct Streams {
   }
 };
 
+// Instances grouped by (N, precision), at most kMaxBatch per group, in order
+// of first appearance; with `group` false every instance is its own group.
+std::vector<std::vector<int>> make_groups(spm_ctx *const *ctx, int n, bool group) {
+  std::vector<std::vector<int>> g;
+  for (int i = 0; i < n; i++) {
+    bool placed = false;
+    if (group)
+      for (auto &grp : g)
+        if ((int)grp.size() < kMaxBatch && ctx[grp[0]]->N == ctx[i]->N && ctx[grp[0]]->prec == ctx[i]->prec) {
+          grp.push_back(i);
+          placed = true;
+          break;
+        }
+    if (!placed) g.push_back({i});
+  }
+  return g;
+}
+
+// K gated steps of one group on its leader's stream.
+int group_steps(spm_ctx *const *ctx, void *const *phi, void *const *uh, const std::vector<int> &grp, int K) {
+  if (grp.size() == 1) return spm_table_of(ctx[grp[0]])->grad_steps(ctx[grp[0]], phi[grp[0]], uh[grp[0]], K);
+  std::vector<spm_ctx *> c;
+  std::vector<void *> p, u;
+  for (int i : grp) {
+    c.push_back(ctx[i]);
+    p.push_back(phi[i]);
+    u.push_back(uh[i]);
+  }
+  return spm_table_of(c[0])->grad_steps_group(c.data(), p.data(), u.data(), (int)grp.size(), K);
+}
+
 // Runs the flows of n contexts to tol (or max_steps each); steps[i] += done.
 // With stall > 0 an instance is also stopped (between graph launches) once
 // `stall` of its steps have brought no new minimum of ||grad F|| (the FP32
@@ -43,15 +79,17 @@ struct Streams {
 // caps (may be null) gives each instance its own step budget (<= max_steps).
 int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int max_steps, double tol, int K,
               int *steps, int stall = 0, const int *caps = nullptr) {
+  const auto groups = make_groups(ctx, n, ctx[0]->batch_group != 0);
+  const int ng = (int)groups.size();
   Streams st;
-  st.s.resize(n + 1);
-  st.ev.resize(n + 1);
-  for (int i = 0; i <= n; i++) {
+  st.s.resize(ng + 1);
+  st.ev.resize(ng + 1);
+  for (int i = 0; i <= ng; i++) {
     if (cudaStreamCreateWithFlags(&st.s[i], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&st.ev[i], cudaEventDisableTiming) != cudaSuccess)
       return spm_fail(SPM_ERR_CUDA, "batch streams");
   }
-  cudaStream_t s0 = st.s[n];
+  cudaStream_t s0 = st.s[ng];
   std::vector<cudaStream_t> saved(n);
   for (int i = 0; i < n; i++) {
     saved[i] = ctx[i]->stream;
@@ -62,25 +100,22 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     ctx[i]->m.tol_grad = tol;
     ctx[i]->m.max_steps = caps ? caps[i] : max_steps;
   }
-  // one step of every instance outside the capture sets up kernel attributes
+  // one step of every group outside the capture sets up kernel attributes
   // and tensor maps; it counts as the first step of the flow
-  for (int i = 0; i < n; i++) {
-    ctx[i]->stream = s0;
-    SPM_TRY(spm_table_of(ctx[i])->grad_step(ctx[i], phi[i], uh[i]));
-  }
+  for (int i = 0; i < n; i++) ctx[i]->stream = s0;
+  for (const auto &grp : groups) SPM_TRY(group_steps(ctx, phi, uh, grp, 1));
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaError_t e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) return spm_fail_cuda(e, "graph capture");
-  e = cudaEventRecord(st.ev[n], s0);
+  e = cudaEventRecord(st.ev[ng], s0);
   int rc = SPM_OK;
-  for (int i = 0; i < n && rc == SPM_OK && e == cudaSuccess; i++) {
-    e = cudaStreamWaitEvent(st.s[i], st.ev[n], 0);
-    ctx[i]->stream = st.s[i];
-    const OpsTable *t = spm_table_of(ctx[i]);
-    rc = t->grad_steps(ctx[i], phi[i], uh[i], K);
-    if (e == cudaSuccess) e = cudaEventRecord(st.ev[i], st.s[i]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, st.ev[i], 0);
+  for (int g = 0; g < ng && rc == SPM_OK && e == cudaSuccess; g++) {
+    e = cudaStreamWaitEvent(st.s[g], st.ev[ng], 0);
+    for (int i : groups[g]) ctx[i]->stream = st.s[g];
+    rc = group_steps(ctx, phi, uh, groups[g], K);
+    if (e == cudaSuccess) e = cudaEventRecord(st.ev[g], st.s[g]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, st.ev[g], 0);
   }
   cudaError_t e2 = cudaStreamEndCapture(s0, &graph);
   if (rc != SPM_OK) {

@@ -474,18 +474,33 @@ struct KParams {
   int xg_cap;
   int xg_regions;
   int nb;
+  // Launches that batch independent instances of one grid size (gradient
+  // chains of a batched relaxation) set `batched`: field b then takes its
+  // model, symbol table, flow words and step records from the arrays below
+  // instead of m, gtab, flow and stats.
+  int batched;
+  ModelC mb[kMaxBatch];
+  const double4 *gtabs[kMaxBatch];
+  int *flows[kMaxBatch];
+  double *statss[kMaxBatch];
 };
 
+// Per-field views of the model, symbols, flow words and records (see `batched`).
+__device__ __forceinline__ const ModelC &model(const KParams &p, int b) { return p.batched ? p.mb[b] : p.m; }
+__device__ __forceinline__ const double4 *gtab_of(const KParams &p, int b) { return p.batched ? p.gtabs[b] : p.gtab; }
+__device__ __forceinline__ int *flow_of(const KParams &p, int b) { return p.batched ? p.flows[b] : p.flow; }
+__device__ __forceinline__ double *stats_of(const KParams &p, int b) { return p.batched ? p.statss[b] : p.stats; }
+
 // Spectral symbols of wave vector (Kx, Ky, Kz) from the per-context table.
-__device__ __forceinline__ double4 symbols(const KParams &p, int Kx, int Ky, int Kz) {
-  const double2 *t = reinterpret_cast<const double2 *>(p.gtab) + 2 * (Kx * Kx + Ky * Ky + Kz * Kz);
+__device__ __forceinline__ double4 symbols(const KParams &p, int Kx, int Ky, int Kz, int b = 0) {
+  const double2 *t = reinterpret_cast<const double2 *>(gtab_of(p, b)) + 2 * (Kx * Kx + Ky * Ky + Kz * Kz);
   const double2 a = __ldg(t), c = __ldg(t + 1);
   return make_double4(a.x, a.y, c.x, c.y);
 }
 
 // Half `h` of the symbols at K^2 (h = 0: {G, 1/(1+dt G)}, h = 1: {1/(G+|Tau|+0.02), 1/(1+G)}).
-__device__ __forceinline__ double2 symbols_half(const KParams &p, int k2, int h) {
-  return __ldg(reinterpret_cast<const double2 *>(p.gtab) + 2 * k2 + h);
+__device__ __forceinline__ double2 symbols_half(const KParams &p, int k2, int h, int b = 0) {
+  return __ldg(reinterpret_cast<const double2 *>(gtab_of(p, b)) + 2 * k2 + h);
 }
 
 // Signed wave number of index i on an N grid (Initialization.cpp:97-107).

@@ -77,8 +77,14 @@ __device__ __forceinline__ unsigned char *smem_base128(unsigned char *raw) {
   return raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
 }
 
-__device__ __forceinline__ bool flow_stopped(const KParams &p) {
-  return p.flow != nullptr && *((volatile const int *)p.flow + FW_GO) == 0;
+__device__ __forceinline__ bool flow_stopped(const KParams &p, int b) {
+  const int *f = flow_of(p, b);
+  return f != nullptr && *((volatile const int *)f + FW_GO) == 0;
+}
+// The step's stop is armed (FW_PENDING, set by its pencil pass before launch).
+__device__ __forceinline__ bool flow_pending(const KParams &p, int b) {
+  const int *f = flow_of(p, b);
+  return f != nullptr && *((volatile const int *)f + FW_PENDING) != 0;
 }
 
 // This CTA's global exchange area in region e (e = 0: inverse exchange, 1:
@@ -452,7 +458,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
-  if (flow_stopped(p)) return;
+  if (flow_stopped(p, blockIdx.y)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -558,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
   double *red = reinterpret_cast<double *>(bars + 2);
   double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbol buffers (one or two tiles)
   __shared__ int s_err;
-  if (flow_stopped(p)) return;
+  if (flow_stopped(p, blockIdx.y)) return;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
@@ -582,7 +588,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
   constexpr int SYMB = pencil_sym_bufs<N, T>(NST, USE_SYM);
   auto sym_stage = [&](int tl, double2 *dst) {
     const int tt = tl / NCH, cz = (tl % NCH) * 8;
-    const double2 *g = reinterpret_cast<const double2 *>(p.gtab) + (USE_SYM ? Op::SYM : 0);
+    const double2 *g = reinterpret_cast<const double2 *>(gtab_of(p, b)) + (USE_SYM ? Op::SYM : 0);
     for (int e = tid; e < SYMN; e += kThreads) {
       const int row = e / KXS, a = e - row * KXS;
       const int kz = row < 8 ? cz + row : N / 2;
@@ -649,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
         return double2{0.0, 0.0};
       } else {
         if (t != 0) return sym_cur[row * KXS + (Kx < 0 ? -Kx : Kx)];
-        return symbols_half(p, Kx * Kx + Ky * Ky + Kz * Kz, Op::SYM);
+        return symbols_half(p, Kx * Kx + Ky * Ky + Kz * Kz, Op::SYM, b);
       }
     };
 
@@ -810,7 +816,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_kernel(const __grid_con
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
-  if (flow_stopped(p)) return;
+  if (flow_stopped(p, blockIdx.y)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
   const int tid = threadIdx.x;
@@ -907,9 +913,9 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_kernel(const __grid
   T2 *buf = ztw + N / 2;
   uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
   double *red = reinterpret_cast<double *>(bar + 2);
-  if (flow_stopped(p)) return;
+  if (flow_stopped(p, blockIdx.y)) return;
   // uniform over the grid: set by the pencil pass of this step, before launch
-  const bool stop = p.flow != nullptr && *((volatile const int *)p.flow + FW_PENDING) != 0;
+  const bool stop = flow_pending(p, blockIdx.y);
 
   cg::cluster_group cluster = cg::this_cluster();
   const int tid = threadIdx.x;
@@ -1033,8 +1039,8 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_pipe_kernel(const _
   T2 *buf = ztw + N / 2;
   uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
   double *red = reinterpret_cast<double *>(bar + 2);
-  if (flow_stopped(p)) return;
-  const bool stop = p.flow != nullptr && *((volatile const int *)p.flow + FW_PENDING) != 0;
+  if (flow_stopped(p, blockIdx.y)) return;
+  const bool stop = flow_pending(p, blockIdx.y);
 
   cg::cluster_group cluster = cg::this_cluster();
   const int tid = threadIdx.x;

@@ -39,14 +39,15 @@ template <class T> struct ProGrad {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
   static constexpr bool FACC = true;
-  template <class A> __device__ static c2<T> pro(const KParams &p, int, size_t, c2<T> x, A (&acc)[1]) {
-    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
-    const T mtau2 = (T)(-0.5 * p.m.Tau), mgam3 = (T)(-p.m.Gamma / 3.0);
+  template <class A> __device__ static c2<T> pro(const KParams &p, int b, size_t, c2<T> x, A (&acc)[1]) {
+    const ModelC &m = model(p, b);
+    const T tau = (T)m.Tau, gam = (T)m.Gamma;
+    const T mtau2 = (T)(-0.5 * m.Tau), mgam3 = (T)(-m.Gamma / 3.0);
     acc[0] += (A)poly_energy(x.x, mtau2, mgam3) + (A)poly_energy(x.y, mtau2, mgam3);
     return c2<T>{poly_force(x.x, tau, gam), poly_force(x.y, tau, gam)};
   }
   __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
-    scal_of(p, b)[SC_E2] = tot[0] * p.m.inv_n3;
+    scal_of(p, b)[SC_E2] = tot[0] * model(p, b).inv_n3;
   }
 };
 
@@ -202,11 +203,11 @@ template <class T> struct OpGrad {
   static constexpr unsigned MAXM = 0x2;
   static constexpr bool FACC = true;
   template <class A>
-  __device__ static void point(const KParams &p, int, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T> s, c2<T> &so,
-                               c2<T> &inv, A (&acc)[3], double w) {
+  __device__ static void point(const KParams &p, int b, int Kx, int Ky, int Kz, double2 sy, c2<T> f, c2<T> s,
+                               c2<T> &so, c2<T> &inv, A (&acc)[3], double w) {
     const A G = (A)sy.x;
-    const T dt = (T)p.m.dt;
-    const c2<T> fh = cscale(f, (T)p.m.inv_n3);
+    const T dt = (T)model(p, b).dt;
+    const c2<T> fh = cscale(f, (T)model(p, b).inv_n3);
     const T iden = (T)sy.y;  // 1 / (1 + dt G)
     c2<T> u1 = {(dt * fh.x + s.x) * iden, (dt * fh.y + s.y) * iden};
     const bool k0 = (Kx == 0 && Ky == 0 && Kz == 0);
@@ -230,18 +231,20 @@ template <class T> struct OpGrad {
     sc[SC_E1] = tot[0];
     sc[SC_RES] = tot[1];
     sc[SC_GN2] = tot[2];
-    if (p.flow) {
-      const int it = p.flow[FW_ITER];
-      if (p.stats) {
-        p.stats[4 * it + 0] = E;
-        p.stats[4 * it + 1] = tot[1];
-        p.stats[4 * it + 2] = gn;
-        p.stats[4 * it + 3] = tot[0];
+    int *flow = flow_of(p, b);
+    if (flow) {
+      const ModelC &m = model(p, b);
+      double *stats = stats_of(p, b);
+      const int it = flow[FW_ITER];
+      if (stats) {
+        stats[4 * it + 0] = E;
+        stats[4 * it + 1] = tot[1];
+        stats[4 * it + 2] = gn;
+        stats[4 * it + 3] = tot[0];
       }
-      p.flow[FW_ITER] = it + 1;
-      if (!(tot[1] > 1e-16) || (p.m.tol_grad > 0 && gn <= p.m.tol_grad) ||
-          (p.m.max_steps > 0 && it + 1 >= p.m.max_steps))
-        p.flow[FW_PENDING] = 1;
+      flow[FW_ITER] = it + 1;
+      if (!(tot[1] > 1e-16) || (m.tol_grad > 0 && gn <= m.tol_grad) || (m.max_steps > 0 && it + 1 >= m.max_steps))
+        flow[FW_PENDING] = 1;
     }
   }
 };
@@ -361,8 +364,9 @@ template <class T> struct EpiFlow {
   static constexpr int NR = 1;
   static constexpr unsigned MAXM = 0;
   __device__ static c2<T> epi(const KParams &, int, size_t, c2<T> y, double (&)[1]) { return y; }
-  __device__ static void fin(const KParams &p, int, const double (&)[1]) {
-    if (p.flow && p.flow[FW_PENDING]) p.flow[FW_GO] = 0;
+  __device__ static void fin(const KParams &p, int b, const double (&)[1]) {
+    int *flow = flow_of(p, b);
+    if (flow && flow[FW_PENDING]) flow[FW_GO] = 0;
   }
 };
 

@@ -388,6 +388,71 @@ template <int N, class T> struct Impl {
   }
   static int grad_steps(spm_ctx *c, void *phi, void *uhat, int K) { return grad_steps_ev(c, phi, uhat, K, nullptr); }
 
+  // K gated steps of n <= kMaxBatch independent instances of this grid size
+  // and precision as one chain of batched launches: one launch per pass
+  // covers every instance (blockIdx.y = instance). Instance b keeps its own
+  // fields, scratch, model, symbol table, flow words and step records
+  // (ctx[b]); the partial sums, tickets and scalars use one slot per instance
+  // in ctx[0]'s buffers, and ctx[0]'s stream, tuning and tensor-map cache
+  // serve the launches. A stopped instance's CTAs return at once. The
+  // per-instance arithmetic is that of grad_steps on its own context, but the
+  // plane kernels exchange through distributed shared memory (the L2 areas
+  // are per context), and results carry the reduction order of a launch of
+  // this size.
+  static int grad_steps_group(spm_ctx *const *ctx, void *const *phi, void *const *uhat, int n, int K) {
+    if (n < 1 || n > kMaxBatch) return spm_fail(SPM_ERR_ARG, "a group holds 1 to 16 instances");
+    spm_ctx *c = ctx[0];
+    for (int b = 0; b < n; b++) {
+      if (ctx[b]->N != N || ctx[b]->prec != c->prec) return spm_fail(SPM_ERR_ARG, "a group shares N and precision");
+      SPM_NEED_SCRATCH(ctx[b], 1);
+    }
+    if (K <= 0) return 0;
+    auto base = [&]() {
+      KParams p = spm_params(c);
+      p.batched = 1;
+      for (int b = 0; b < n; b++) {
+        p.mb[b] = ctx[b]->m;
+        p.gtabs[b] = reinterpret_cast<const double4 *>(ctx[b]->gtab);
+        p.flows[b] = ctx[b]->flow;
+        p.statss[b] = ctx[b]->stats;
+      }
+      return p;
+    };
+    auto head = [&]() {
+      KParams p = base();
+      for (int b = 0; b < n; b++) {
+        p.in[b] = phi[b];
+        p.out[b] = spm_bufA(ctx[b], 0);
+      }
+      return plane_fwd<N, T, ProGrad<T>>(c, p, n);
+    };
+    SPM_TRY(head());
+    for (int k = 0; k < K; k++) {
+      KParams q = base();
+      for (int b = 0; b < n; b++) {
+        q.in[b] = spm_bufA(ctx[b], 0);
+        q.st[b] = uhat[b];
+        q.sto[b] = uhat[b];
+        q.out[b] = spm_bufB(ctx[b], 0);
+      }
+      SPM_TRY((pencil<N, T, OpGrad<T>>(c, q, n)));
+      KParams r = base();
+      for (int b = 0; b < n; b++) r.in[b] = spm_bufB(ctx[b], 0);
+      if (c->fuse_planes && k + 1 < K) {
+        for (int b = 0; b < n; b++) {
+          r.out[b] = spm_bufA(ctx[b], 0);
+          r.sto[b] = phi[b];
+        }
+        SPM_TRY((plane_inv_fwd<N, T, EpiFlow<T>, ProGrad<T>>(c, r, n)));
+      } else {
+        for (int b = 0; b < n; b++) r.out[b] = phi[b];
+        SPM_TRY((plane_inv<N, T, EpiFlow<T>>(c, r, n)));
+        if (k + 1 < K) SPM_TRY(head());
+      }
+    }
+    return 0;
+  }
+
   // -grad F(phi) -> grad, ||grad||^2 -> scal[SC_GN2]
   static int ngrad(spm_ctx *c, const void *phi, void *grad) {
     SPM_NEED_SCRATCH(c, 1);
@@ -542,7 +607,7 @@ template <int N, class T> struct Impl {
 
   static const OpsTable *table() {
     static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_steps_ev, &grad_step_ev, &ngrad, &hv, &precond, &dot,
-                               &tangent, &force, &gnorm, &hisd_step};
+                               &tangent, &force, &gnorm, &hisd_step, &grad_steps_group};
     return &t;
   }
 };

@@ -379,6 +379,11 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->plane_xg = value;
     return spm_ensure_xg(c);
   }
+  if (std::strcmp(knob, "batch_group") == 0) {
+    if (value != 0 && value != 1) return spm_fail(SPM_ERR_ARG, "batch_group must be 0 or 1");
+    c->batch_group = value;
+    return SPM_OK;
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
@@ -387,6 +392,7 @@ extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (std::strcmp(knob, "plane_cps") == 0) return c->plane_cps;
   if (std::strcmp(knob, "fuse_planes") == 0) return c->fuse_planes;
   if (std::strcmp(knob, "plane_xg") == 0) return c->plane_xg;
+  if (std::strcmp(knob, "batch_group") == 0) return c->batch_group;
   return -1;
 }
 
@@ -557,6 +563,7 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->plane_cps = c->plane_cps;
   c->twin->fuse_planes = c->fuse_planes;
   c->twin->plane_xg = c->plane_xg;
+  c->twin->batch_group = c->batch_group;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
   spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg);
   return spm_ensure_xg(c->twin);

@@ -53,6 +53,7 @@ struct spm_ctx {
   int plane_xg = 0;             // gradient-chain plane kernels: exchanges through L2 (spm::kXgFwd | kXgInv bits)
   void *xg = nullptr;           // their global exchange areas (2 x xg_cap CTAs x 16 N complex)
   int xg_cap = 0;
+  int batch_group = 1;          // spm_batch_grad_flow: same-size instances share launches (knob "batch_group")
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
   const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)

@@ -21,6 +21,8 @@ struct OpsTable {
   int (*force)(spm_ctx *, void *const *x, int n, const void *v, const void *vhat, const void *gv, double factor);
   int (*gnorm)(spm_ctx *, const void *const *x, int n);
   int (*hisd_step)(spm_ctx *, void *x, const void *t, void *dx, double beta);
+  // K gated steps of n instances of one grid size and precision, one launch per pass for all
+  int (*grad_steps_group)(spm_ctx *const *ctx, void *const *phi, void *const *uhat, int n, int nsteps);
 };
 
 // prec: 0 = FP64, 1 = FP32

@@ -54,10 +54,14 @@ def test_mixed_flow_matches_fp64_minimum(cuda):
     assert rel(b.cpu().numpy(), a.cpu().numpy()) < 1e-4  # both within ||grad F|| / |Tau| of the minimum
 
 
-def test_batched_flows_match_single_flows(cuda):
+@pytest.mark.parametrize("group", [1, 0])
+def test_batched_flows_match_single_flows(cuda, group):
     """spm_batch_grad_flow over instances of different N and parameters gives,
     per instance, exactly the steps and state of a single flow (deterministic
-    reductions: identical bits alone and in the batch)."""
+    reductions: identical bits alone and in the batch), both when instances of
+    one size share every launch (batch_group 1: three 32^3 instances with
+    different L and Tau in one launch per pass, two 64^3 ones in another) and
+    when each instance has its own launches (batch_group 0)."""
     import ctypes
     import spmiqc
     lib = spmiqc.lib()
@@ -65,10 +69,12 @@ def test_batched_flows_match_single_flows(cuda):
     f.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                   ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                   ctypes.POINTER(ctypes.c_int)]
-    specs = [(32, 26.0, -0.0061, 1), (64, 20.0, -0.01, 2), (96, 28.0, -0.015, 3), (32, 18.0, -0.02, 4)]
+    specs = [(32, 26.0, -0.0061, 1), (64, 20.0, -0.01, 2), (96, 28.0, -0.015, 3), (32, 18.0, -0.02, 4),
+             (64, 29.0, -0.004, 5), (32, 22.5, -0.012, 6)]
     ctxs, phis, uhs, singles = [], [], [], []
     for N, L, tau, seed in specs:
         c = spmiqc.SpmContext(N, L=L, Tau=tau)
+        c.tune("batch_group", group)
         p0 = npo.uniform_field(N, seed)
         p = cuda.from_numpy(p0).cuda()
         ctxs.append(c), phis.append(p), uhs.append(c.my_fft(p))
