@@ -74,8 +74,8 @@ int group_steps(spm_ctx *const *ctx, void *const *phi, void *const *uh, const st
 
 // Runs the flows of n contexts to tol (or max_steps each); steps[i] += done.
 // With stall > 0 an instance is also stopped (between graph launches) once
-// `stall` of its steps have brought no new minimum of ||grad F|| (the FP32
-// rounding floor of a mixed run).
+// FloorWatch (windows of `stall` steps, switch point tol) sees its FP32
+// rounding floor.
 // caps (may be null) gives each instance its own step budget (<= max_steps).
 int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int max_steps, double tol, int K,
               int *steps, int stall = 0, const int *caps = nullptr) {
@@ -129,8 +129,9 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
     return spm_fail_cuda(e, "graph instantiate");
   }
   std::vector<int> host(8 * (size_t)n);
-  std::vector<double> best(n, INFINITY), rec;
-  std::vector<int> seen(n, 1), last_better(n, 0);  // the step outside the graph is record 0
+  std::vector<double> rec;
+  std::vector<int> seen(n, 1);  // the step outside the graph is record 0
+  std::vector<FloorWatch> watch(n, FloorWatch(tol, stall > 0 ? stall : 1));
   static const int kZero = 0;
   const int launches = (max_steps + K - 1) / K;
   for (int l = 0; l < launches && rc == SPM_OK; l++) {
@@ -159,13 +160,10 @@ int run_phase(spm_ctx *const *ctx, void *const *phi, void *const *uh, int n, int
             rc = spm_fail_cuda(e, "batch records");
             break;
           }
-          for (int s = 0; s < it - seen[i]; s++)
-            if (rec[4 * (size_t)s + 2] < best[i]) {
-              best[i] = rec[4 * (size_t)s + 2];
-              last_better[i] = seen[i] + s;
-            }
+          bool stop = false;
+          for (int s = 0; s < it - seen[i] && !stop; s++) stop = watch[i].step(rec[4 * (size_t)s + 2]);
           seen[i] = it;
-          if (it - last_better[i] >= stall) {  // the instance stops before the next launch
+          if (stop) {  // the instance stops before the next launch
             e = cudaMemcpyAsync(ctx[i]->flow + FW_GO, &kZero, sizeof(int), cudaMemcpyHostToDevice, s0);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
             if (e != cudaSuccess) {

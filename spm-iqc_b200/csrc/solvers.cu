@@ -308,6 +308,44 @@ int orth_with_drop(spm_ctx *c, void *const *X, int k, double thr, std::vector<in
   return SPM_OK;
 }
 
+// X (k fields) <- X orthogonalised against Q (nq orthonormal fields, zero
+// fields allowed) and among its own columns in order: block classical
+// Gram-Schmidt with a Cholesky factorisation of the Schur complement, two
+// passes of one Gram [Q X]^T X and one combination [Q X] -> X each (the
+// second re-orthogonalises). In the first pass a column whose norm after
+// projecting out Q and the columns before it is <= thr is dropped (zeroed,
+// keep[j] = 0): the 1e-8 tests of LOBPCG.cpp:298, 319, which follow the same
+// projections (Orthoi_v2V against V (and W), Orthoi_Vi against the earlier
+// columns) one column at a time.
+int block_orth(spm_ctx *c, void *const *Q, int nq, void *const *X, int k, double thr, std::vector<int> &keep) {
+  std::vector<void *> QX(Q, Q + nq);
+  QX.insert(QX.end(), X, X + k);
+  const int m = nq + k;
+  std::vector<double> G, S((size_t)k * k), B, Cf;
+  for (int pass = 0; pass < 2; pass++) {
+    SPM_TRY(gram(c, QX.data(), m, X, k, G));  // G[a * k + j] = <QX_a, X_j>
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++) {
+        double v = G[(size_t)(nq + i) * k + j];
+        for (int q = 0; q < nq; q++) v -= G[(size_t)q * k + i] * G[(size_t)q * k + j];
+        S[(size_t)i * k + j] = v;
+      }
+    gs_coefficients(S, k, pass == 0 ? thr : 0.0, keep, B);
+    // X_new = X B - Q (C B), C = Q^T X
+    Cf.assign((size_t)m * k, 0.0);
+    for (int q = 0; q < nq; q++)
+      for (int j = 0; j < k; j++) {
+        double v = 0.0;
+        for (int l = 0; l < k; l++) v += G[(size_t)q * k + l] * B[(size_t)l * k + j];
+        Cf[(size_t)q * k + j] = -v;
+      }
+    for (int l = 0; l < k; l++)
+      for (int j = 0; j < k; j++) Cf[(size_t)(nq + l) * k + j] = B[(size_t)l * k + j];
+    SPM_TRY(combine(c, QX.data(), m, X, k, Cf, nullptr, false));
+  }
+  return SPM_OK;
+}
+
 int zero_fields(spm_ctx *c, void *dst, int k) {
   cudaError_t e = cudaMemsetAsync(dst, 0, c->field_bytes * (size_t)k, c->stream);
   return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "zero");
@@ -424,6 +462,70 @@ static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::v
 static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &have_p, void *const *V0 = nullptr,
                       int k0 = 0) {
   std::vector<double> G;
+  if (k0 == 0) {
+    // W: preconditioned residuals against V and in order, P against [V W],
+    // each by two block Gram-Schmidt passes; then Rayleigh-Ritz on [V W P]
+    SPM_TRY(precond_many(c, B.W.data(), k));
+    std::vector<int> keepW(k, 1), keepP(k, 0);
+    SPM_TRY(block_orth(c, B.Vc.data(), k, B.W.data(), k, 1e-8, keepW));
+    SPM_TRY(hv_many(c, phi, B.W.data(), B.Y.data(), k));
+    if (have_p) {
+      std::vector<void *> VW(2 * k);
+      for (int i = 0; i < k; i++) {
+        VW[i] = B.Vc[i];
+        VW[k + i] = B.W[i];
+      }
+      keepP.assign(k, 1);
+      SPM_TRY(block_orth(c, VW.data(), 2 * k, B.P.data(), k, 1e-8, keepP));
+      SPM_TRY(hv_many(c, phi, B.P.data(), B.Up.data(), k));
+    }
+    std::vector<void *> S, HS;
+    for (int i = 0; i < k; i++) {
+      S.push_back(B.Vc[i]);
+      HS.push_back(B.U[i]);
+    }
+    for (int i = 0; i < k; i++)
+      if (keepW[i]) {
+        S.push_back(B.W[i]);
+        HS.push_back(B.Y[i]);
+      }
+    for (int i = 0; i < k; i++)
+      if (keepP[i]) {
+        S.push_back(B.P[i]);
+        HS.push_back(B.Up[i]);
+      }
+    const int m = (int)S.size();
+    SPM_TRY(gram(c, S.data(), m, HS.data(), m, G));
+    std::vector<double> Gs((size_t)m * m), vals, vecs;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < m; j++) Gs[(size_t)i * m + j] = (G[(size_t)j * m + i] + G[(size_t)i * m + j]) * 0.5;
+    sym_eig(Gs, m, vals, vecs);
+    std::vector<double> C((size_t)m * k);
+    for (int p = 0; p < m; p++)
+      for (int q = 0; q < k; q++) C[(size_t)p * k + q] = vecs[(size_t)p * m + q];
+    SPM_TRY(combine(c, S.data(), m, B.Vn.data(), k, C, nullptr, false));
+    std::swap(B.P, B.Vc);   // P holds the old V
+    std::swap(B.Vc, B.Vn);  // V holds the new block
+    have_p = true;
+    // each row minus its mean, then Gram-Schmidt (LOBPCG.cpp:443-449), in one
+    // pass: <V_i - mu_i, V_j - mu_j> = <V_i, V_j> - mu_i mu_j, and the
+    // combination subtracts mu B from B's columns (the Ritz block is already
+    // orthonormal to rounding, so one Cholesky pass suffices)
+    std::vector<double> mu, Bc;
+    SPM_TRY(means(c, B.Vc.data(), k, mu));
+    SPM_TRY(gram(c, B.Vc.data(), k, B.Vc.data(), k, G));
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++) G[(size_t)i * k + j] -= mu[i] * mu[j];
+    std::vector<int> keep(k, 1);
+    gs_coefficients(G, k, 0.0, keep, Bc);
+    for (int j = 0; j < k; j++)
+      if (!keep[j]) return spm_fail(SPM_ERR_NONFINITE, "block vectors are linearly dependent");
+    std::vector<double> d(k, 0.0);
+    for (int j = 0; j < k; j++)
+      for (int p = 0; p < k; p++) d[j] -= mu[p] * Bc[(size_t)p * k + j];
+    return combine(c, B.Vc.data(), k, B.Vc.data(), k, Bc, &d, false);
+  }
+  // with fixed fields V0 (GOSD): the projections one block at a time
   SPM_TRY(precond_many(c, B.W.data(), k));
   SPM_TRY(project_out(c, B.Vc.data(), k, B.W.data(), k));
   if (k0 > 0) SPM_TRY(project_out(c, V0, k0, B.W.data(), k));
@@ -646,11 +748,11 @@ extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int 
   if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
   int n32 = 0, n64 = 0;
   const double sw = switch_tol > tol ? switch_tol : tol;
-  // FP32 in windows of kWindow iterations until res <= sw, or until a window
-  // brings no new minimum of res (the FP32 rounding floor is reached)
+  // FP32 in windows of kWindow iterations until res <= sw, or until FP32
+  // stops making progress (its rounding floor, FloorWatch)
   constexpr int kWindow = 256;
   std::vector<double> rec(kWindow);
-  double best = INFINITY;
+  FloorWatch watch(sw, kWindow);
   while (n32 < maxiter) {
     const int chunk = std::min(kWindow, maxiter - n32);
     int done = 0;
@@ -658,10 +760,9 @@ extern "C" int spm_spring_pairing_mixed(spm_ctx *c, void *phi0, void *phi1, int 
     SPM_TRY(spm_spring_pairing(c->twin, a, b, chunk, sw, out, &done));
     n32 += done;
     if (done == 0 || done < chunk || out[done - 1] <= sw) break;
-    double wmin = INFINITY;
-    for (int i = 0; i < done; i++) wmin = std::min(wmin, out[i]);
-    if (!(wmin < best)) break;
-    best = wmin;
+    bool stop = false;
+    for (int i = 0; i < done && !stop; i++) stop = watch.step(out[i]);
+    if (stop) break;
   }
   c->launches += c->twin->launches + 2;
   c->twin->launches = 0;

@@ -551,6 +551,25 @@ extern "C" int spm_grad_flow(spm_ctx *c, void *phi, void *uhat, int max_steps, d
   return spm_grad_flow_collect(c, stats, max_steps, steps_done);
 }
 
+FloorWatch::FloorWatch(double switch_at, int window) : sw(switch_at), short_win(window), long_win(16 * window) {}
+
+// One more FP32 residual; true when the FP32 phase should hand over to FP64.
+// A new best counts only if it is 0.5 % below the previous one. Flows are
+// not monotone at first (a structure forming from a random field can raise
+// ||grad F|| for thousands of steps), so a short stall (short_win residuals
+// without a new best) ends the phase only once the best is within 10x of the
+// switch point; anywhere, a long stall (long_win residuals) ends it.
+bool FloorWatch::step(double r) {
+  n++;
+  if (r < 0.995 * best) {
+    best = r;
+    last = n;
+    return false;
+  }
+  const int since = n - last;
+  return (best < 10.0 * sw && since >= short_win) || since >= long_win;
+}
+
 int spm_ensure_twin(spm_ctx *c) {
   if (!c->twin) {
     const size_t n = (size_t)c->N * c->N * c->N;
@@ -588,11 +607,11 @@ extern "C" int spm_grad_flow_mixed(spm_ctx *c, void *phi, void *uhat, int max_st
   if (e != cudaSuccess) return spm_fail_cuda(e, "cast");
   int n32 = 0, n64 = 0;
   const double sw = switch_tol > tol_grad ? switch_tol : tol_grad;
-  // FP32 in windows of kWindow steps until ||grad F|| <= sw, or until a window
-  // brings no new minimum of ||grad F|| (the FP32 rounding floor is reached).
+  // FP32 in windows of kWindow steps until ||grad F|| <= sw, or until FP32
+  // stops making progress (its rounding floor): see FloorWatch.
   constexpr int kWindow = 512;
   std::vector<spm_step_stats> rec(kWindow);
-  double best = INFINITY;
+  FloorWatch watch(sw, kWindow);
   while (n32 < max_steps) {
     const int chunk = std::min(kWindow, max_steps - n32);
     int done = 0;
@@ -600,11 +619,10 @@ extern "C" int spm_grad_flow_mixed(spm_ctx *c, void *phi, void *uhat, int max_st
     SPM_TRY(spm_grad_flow(c->twin, phi32, uh32, chunk, sw, out, &done));
     n32 += done;
     if (done == 0) break;
-    double wmin = INFINITY;
-    for (int i = 0; i < done; i++) wmin = std::min(wmin, out[i].grad_norm);
     if (done < chunk || out[done - 1].grad_norm <= sw || out[done - 1].res <= 1e-16) break;
-    if (!(wmin < best)) break;
-    best = wmin;
+    bool stop = false;
+    for (int i = 0; i < done && !stop; i++) stop = watch.step(out[i].grad_norm);
+    if (stop) break;
   }
   c->launches += c->twin->launches;
   c->twin->launches = 0;

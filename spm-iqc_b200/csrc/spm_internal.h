@@ -79,6 +79,16 @@ void spm_free_extra(spm_ctx *c);
 // Creates (once) the FP32 twin context and its two FP32 fields, and binds it
 // to the context's stream, cancel flag and tuning.
 int spm_ensure_twin(spm_ctx *c);
+// Decides when the FP32 phase of a mixed-precision run has reached its
+// rounding floor, from its sequence of residuals (||grad F|| or the SPM
+// residual); switch_at is the residual at which the phase hands over anyway.
+struct FloorWatch {
+  double sw, best = 1e300;
+  int short_win, long_win, n = 0, last = 0;
+  FloorWatch(double switch_at, int window);
+  bool step(double r);
+};
+
 // The autotuner's remembered choice for (device, N, precision), if any.
 bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg);
 const struct OpsTable *spm_table_of(const spm_ctx *c);
