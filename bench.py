@@ -675,7 +675,7 @@ def main():
                          "(fixed kernel variants for ncu captures)")
     ap.add_argument("--serve", action="store_true", help="run the serving workload instead (one JSON line)")
     ap.add_argument("--serve-jobs", type=int, default=40)
-    ap.add_argument("--serve-jobs-default", type=int, default=20,
+    ap.add_argument("--serve-jobs-default", type=int, default=32,
                     help="jobs of the serving leg on the default benchmark line")
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--batch", action="store_true", help="run the batched-relaxation workload instead (one JSON line)")
