@@ -39,7 +39,11 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 // depend on scheduling.
 // U = k-steps loaded per loop iteration, TM = row tiles (8 vectors each) at
 // most per operand: (4, 1), (4, 2) or (2, 3) by block size.
-template <class T, int U, int TM>
+// YT >= 0: Y's fields are X's fields from index 8 YT on (Y_b = X_{8 YT + b}),
+// so a lane's B fragment of tile t is its A fragment of tile t + YT and Y is
+// not read again (the Grams [Q X]^T X of the block orthogonalisations and the
+// X^T X ones); YT = -1: Y is read.
+template <class T, int U, int TM, int YT = -1>
 __global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_constant__ GramP p) {
   __shared__ int s_last;
   if (p.flow && *((volatile const int *)p.flow) == 0) return;
@@ -68,9 +72,15 @@ __global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_cons
       const size_t su = s + u * W;
       const bool in = su < steps;
 #pragma unroll
+      for (int t = 0; t < TM; t++) a[u][t] = (xr[t] && in) ? __ldg(xr[t] + 4 * su + tig) : V2{0, 0};
+#pragma unroll
       for (int t = 0; t < TM; t++) {
-        a[u][t] = (xr[t] && in) ? __ldg(xr[t] + 4 * su + tig) : V2{0, 0};
-        b[u][t] = (yr[t] && in) ? __ldg(yr[t] + 4 * su + tig) : V2{0, 0};
+        if constexpr (YT >= 0) {
+          // the same lane and point mapping as the A fragment; rows beyond mb are not used
+          b[u][t] = (t + YT < TM) ? a[u][t + YT] : V2{0, 0};
+        } else {
+          b[u][t] = (yr[t] && in) ? __ldg(yr[t] + 4 * su + tig) : V2{0, 0};
+        }
       }
     }
 #pragma unroll

@@ -81,13 +81,31 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
   c->launches++;
   // blocks of up to 8 / 16 vectors: four k-steps per loop iteration; up to 24: two
   const int tiles = (std::max(ma, mb) + 7) / 8;
+  // Y = X[8 yt .. 8 yt + mb) (whole tiles): Y's fields are not read again
+  int yt = -1;
+  if (mb % 8 == 0)
+    for (int off = 0; off + mb <= ma && yt < 0; off += 8) {
+      bool same = true;
+      for (int b = 0; b < mb && same; b++) same = (Y[b] == X[off + b]);
+      if (same) yt = off / 8;
+    }
   auto launch = [&](auto kd, auto kf) {
     if (c->prec == SPM_FP64) kd<<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
     else kf<<<kGramBlocks, kGramWarps * 32, 0, c->stream>>>(p);
   };
-  if (tiles == 1) launch(gram_kernel<double, 4, 1>, gram_kernel<float, 4, 1>);
-  else if (tiles == 2) launch(gram_kernel<double, 4, 2>, gram_kernel<float, 4, 2>);
-  else launch(gram_kernel<double, 2, 3>, gram_kernel<float, 2, 3>);
+  if (tiles == 1) {
+    if (yt == 0) launch(gram_kernel<double, 4, 1, 0>, gram_kernel<float, 4, 1, 0>);
+    else launch(gram_kernel<double, 4, 1>, gram_kernel<float, 4, 1>);
+  } else if (tiles == 2) {
+    if (yt == 0) launch(gram_kernel<double, 4, 2, 0>, gram_kernel<float, 4, 2, 0>);
+    else if (yt == 1) launch(gram_kernel<double, 4, 2, 1>, gram_kernel<float, 4, 2, 1>);
+    else launch(gram_kernel<double, 4, 2>, gram_kernel<float, 4, 2>);
+  } else {
+    if (yt == 0) launch(gram_kernel<double, 2, 3, 0>, gram_kernel<float, 2, 3, 0>);
+    else if (yt == 1) launch(gram_kernel<double, 2, 3, 1>, gram_kernel<float, 2, 3, 1>);
+    else if (yt == 2) launch(gram_kernel<double, 2, 3, 2>, gram_kernel<float, 2, 3, 2>);
+    else launch(gram_kernel<double, 2, 3>, gram_kernel<float, 2, 3>);
+  }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->h_gram, s->gram_out, sizeof(double) * ma * mb, cudaMemcpyDeviceToHost, c->stream);
