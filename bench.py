@@ -37,20 +37,24 @@ WORKLOAD = ("grad-flow 256^3 FP64, L=26, Tau=-0.0061, Gamma=0.30, dt=0.3, phi0 =
             "30-vector cosine shell (amp 0.15) + N(0,1e-3) noise")
 
 
-def kernel_traffic():
+def kernel_traffic(schedule=None):
     """DRAM bytes per launch of the step kernels at 256^3 FP64, from the ncu
-    capture summarised in profiles/kernel_traffic_256_fp64.md (lines
-    `traffic <kernel> <bytes>`)."""
-    out = {}
+    captures summarised in profiles/kernel_traffic_256_fp64.md (lines
+    `traffic <kernel> <bytes> <plane_cps,fuse_planes,plane_xg>`): those of the
+    given schedule, else of the first schedule listed."""
+    out, first = {}, {}
+    want = None if schedule is None else f"{schedule['plane_cps']},{schedule['fuse_planes']},{schedule['plane_xg']}"
     try:
         with open(os.path.join(ROOT, "profiles", "kernel_traffic_256_fp64.md")) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) == 3 and parts[0] == "traffic":
-                    out[parts[1]] = int(parts[2])
+                if len(parts) == 4 and parts[0] == "traffic":
+                    first.setdefault(parts[1], int(parts[2]))
+                    if parts[3] == want:
+                        out[parts[1]] = int(parts[2])
     except OSError:
         pass
-    return out
+    return out or first
 
 
 def peaks():
@@ -798,7 +802,7 @@ def main():
     dom = 1 if kms[1] >= kms[2] else 2
     achieved = kern_bytes[dom] / (kms[dom] * 1e-3) / 1e9
     step_bytes = (6 * args.steps + 2) * S / args.steps  # per step of the timed chain
-    traffic = kernel_traffic().get(names[dom])
+    traffic = kernel_traffic(sched64).get(names[dom])
 
     # Hessian-vector products, block of 8 (LOBPCG k = 8)
     V = torch.from_numpy(np.random.default_rng(5).standard_normal((8, N, N, N))).cuda()

@@ -114,7 +114,9 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
       float ms = 0;
       if (rc == SPM_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < t) t = ms;
     }
-    if (rc == SPM_OK && t < best_ms) {
+    // a later candidate must be at least 1 % faster to replace the best so far
+    // (candidates within timing noise of each other resolve to the earlier one)
+    if (rc == SPM_OK && t < 0.99f * best_ms) {
       best_ms = t;
       best = cand;
     }

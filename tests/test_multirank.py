@@ -76,14 +76,19 @@ def test_two_rank_paths_on_gloo():
 
 def test_bench_reads_the_committed_traffic_profile():
     """bench.py's roofline.traffic comes from the committed ncu summary: every
-    chain kernel of the gradient step has a per-launch byte count there, and the
-    fused plane pass and the pencil pass move no more than 10 % above their
-    algorithmic bytes (no re-reads)."""
+    chain kernel of the gradient step has a per-launch byte count there for
+    each captured schedule; with schedule 5 the fused plane pass and the pencil
+    pass move no more than 10 % above their algorithmic bytes (no re-reads),
+    and the pipelined schedule 6 is recorded with its own (larger) traffic."""
     import sys
     sys.path[:0] = [ROOT, os.path.join(ROOT, "spm-iqc_b200")]
     import bench
-    tr = bench.kernel_traffic()
     S = 256 ** 3 * 8
-    assert set(tr) == {"pencil<OpGrad>", "plane_inv_fwd<EpiFlow,ProGrad>", "plane_fwd<ProGrad>", "plane_inv<EpiFlow>"}
+    kernels = {"pencil<OpGrad>", "plane_inv_fwd<EpiFlow,ProGrad>", "plane_fwd<ProGrad>", "plane_inv<EpiFlow>"}
+    tr = bench.kernel_traffic({"plane_cps": 5, "fuse_planes": 1, "plane_xg": 3})
+    assert set(tr) == kernels
     assert 0 < tr["pencil<OpGrad>"] <= 1.1 * 4 * S
     assert 0 < tr["plane_inv_fwd<EpiFlow,ProGrad>"] <= 1.1 * 2 * S
+    t6 = bench.kernel_traffic({"plane_cps": 6, "fuse_planes": 1, "plane_xg": 3})
+    assert set(t6) == kernels and t6["plane_inv_fwd<EpiFlow,ProGrad>"] > tr["plane_inv_fwd<EpiFlow,ProGrad>"]
+    assert bench.kernel_traffic() == tr  # no schedule given: the first one listed
