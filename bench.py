@@ -670,6 +670,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--flow-precision", default="fp64", choices=["fp64", "fp32"],
+                    help="precision of the --only-flow run")
     ap.add_argument("--only-flow", action="store_true",
                     help="run only the warm-up and timed gradient steps (used for ncu captures)")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP64 vs mixed time-to-tolerance leg")
@@ -712,7 +714,9 @@ def main():
     torch.cuda.set_device(local)
     L_ = spmiqc.lib()
     stream = torch.cuda.current_stream()
-    ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp64", stream=stream.cuda_stream)
+    # --only-flow may time the flow in FP32 (for captures of the FP32 kernels)
+    prec = args.flow_precision if args.only_flow else "fp64"
+    ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, prec, stream=stream.cuda_stream)
     # schedule choice by the autotuner, outside the timed region (FP32 too, for
     # the FP32 leg and the FP32 twin of the mixed flow)
     if args.schedule:
@@ -727,7 +731,7 @@ def main():
     sched32 = _c32.tuning()
     _c32.close()
     phi_h = initial_field(1 + rank)
-    phi = torch.from_numpy(phi_h).cuda()
+    phi = torch.from_numpy(phi_h.astype(np.float32) if prec == "fp32" else phi_h).cuda()
     uh = ctx.my_fft(phi)
     S = N ** 3 * 8
 
@@ -774,7 +778,8 @@ def main():
     if args.only_flow:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "steps/s", "steps": args.steps,
-                              "warmup": args.warmup, "gpu_launches": int(launches), "only_flow": True}))
+                              "warmup": args.warmup, "gpu_launches": int(launches), "only_flow": True,
+                              "precision": prec, "schedule": ctx.tuning()}))
         ctx.close()
         return 0
 
