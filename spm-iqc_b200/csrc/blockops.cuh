@@ -121,23 +121,33 @@ __global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_cons
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  for (int e = threadIdx.x; e < p.ma * p.mb; e += blockDim.x) {
+  // grid total of every entry in a fixed order: each warp takes entries in
+  // turn, lane l sums the partials of CTAs l, l + 32, ... (independent loads
+  // in flight), then a fixed butterfly over the lanes
+  for (int e = warp; e < p.ma * p.mb; e += kGramWarps) {
     const int r = e / p.mb, c = e % p.mb;
     double s = 0.0;
-    for (unsigned bk = 0; bk < gridDim.x; bk++) s += __ldcg(p.partials + (size_t)bk * kBlkMax * kBlkMax + r * kBlkMax + c);
-    p.out[e] = s * p.inv_n;
+#pragma unroll 4
+    for (unsigned bk = lane; bk < gridDim.x; bk += 32)
+      s += __ldcg(p.partials + (size_t)bk * kBlkMax * kBlkMax + r * kBlkMax + c);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) p.out[e] = s * p.inv_n;
   }
   if (threadIdx.x == 0) *p.ticket = 0u;
 }
 
+// The coefficients travel in the kernel parameters (6.3 KB), so a
+// combination needs no host-to-device copy (and no stream synchronisation
+// for one) before its launch.
 struct CombP {
   const void *X[kBlkMax + 8];
   void *Y[kBlkMax];
   int nin, nout;
   size_t n;
-  const double *C;   // nin x nout, row-major: Y_q += C[p*nout + q] X_p
-  const double *d;   // nout constants or null
-  int accumulate;    // Y_q = (accumulate ? Y_q : 0) + ...
+  double C[(kBlkMax + 8) * kBlkMax];  // nin x nout, row-major: Y_q += C[p*nout + q] X_p
+  double d[kBlkMax];                  // nout constants (zeros when none)
+  int accumulate;                     // Y_q = (accumulate ? Y_q : 0) + ...
   const int *flow;
 };
 
@@ -170,7 +180,7 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
   __shared__ double sc[(kBlkMax + 8) * kBlkMax + kBlkMax];
   if (p.flow && *((volatile const int *)p.flow) == 0) return;
   for (int e = threadIdx.x; e < p.nin * p.nout; e += blockDim.x) sc[e] = p.C[e];
-  for (int e = threadIdx.x; e < p.nout; e += blockDim.x) sc[(kBlkMax + 8) * kBlkMax + e] = p.d ? p.d[e] : 0.0;
+  for (int e = threadIdx.x; e < p.nout; e += blockDim.x) sc[(kBlkMax + 8) * kBlkMax + e] = p.d[e];
   __syncthreads();
   const double *dd = sc + (kBlkMax + 8) * kBlkMax;
   const size_t nv = p.n / PTS;

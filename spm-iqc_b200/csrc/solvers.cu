@@ -33,7 +33,6 @@ struct Solver {
   double *gram_part = nullptr;  // [kGramBlocks][kBlkMax^2]
   unsigned *gram_ticket = nullptr;
   double *gram_out = nullptr;   // kBlkMax^2
-  double *coef = nullptr;       // (kBlkMax + 8) * kBlkMax + kBlkMax
   double *h_gram = nullptr;     // pinned
   void *lob = nullptr;          // LOBPCG work fields: U, W, Y, P, Up, Vn (k each)
   int lob_k = 0;
@@ -55,7 +54,6 @@ int ensure_base(spm_ctx *c) {
   if (e == cudaSuccess) e = cudaMalloc(&s->gram_ticket, sizeof(unsigned) * 4);
   if (e == cudaSuccess) e = cudaMemset(s->gram_ticket, 0, sizeof(unsigned) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->gram_out, sizeof(double) * kBlkMax * kBlkMax);
-  if (e == cudaSuccess) e = cudaMalloc(&s->coef, sizeof(double) * ((kBlkMax + 8) * kBlkMax + kBlkMax));
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_gram, sizeof(double) * kBlkMax * kBlkMax);
   if (e != cudaSuccess) return spm_fail_cuda(e, "solver buffers");
   return SPM_OK;
@@ -101,9 +99,10 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
     else if (yt == 1) launch(gram_kernel<double, 4, 2, 1>, gram_kernel<float, 4, 2, 1>);
     else launch(gram_kernel<double, 4, 2>, gram_kernel<float, 4, 2>);
   } else {
-    if (yt == 0) launch(gram_kernel<double, 2, 3, 0>, gram_kernel<float, 2, 3, 0>);
-    else if (yt == 1) launch(gram_kernel<double, 2, 3, 1>, gram_kernel<float, 2, 3, 1>);
-    else if (yt == 2) launch(gram_kernel<double, 2, 3, 2>, gram_kernel<float, 2, 3, 2>);
+    // with Y aliased the B fragments take no registers of their own: four k-steps
+    if (yt == 0) launch(gram_kernel<double, 4, 3, 0>, gram_kernel<float, 4, 3, 0>);
+    else if (yt == 1) launch(gram_kernel<double, 4, 3, 1>, gram_kernel<float, 4, 3, 1>);
+    else if (yt == 2) launch(gram_kernel<double, 4, 3, 2>, gram_kernel<float, 4, 3, 2>);
     else launch(gram_kernel<double, 2, 3>, gram_kernel<float, 2, 3>);
   }
   cudaError_t e = cudaGetLastError();
@@ -120,15 +119,7 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
 // Y_q = (acc ? Y_q : 0) + sum_p C[p*nout + q] X_p + d[q]
 int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const std::vector<double> &C,
             const std::vector<double> *d, bool acc) {
-  Solver *s = solver(c);
   if (nin > kBlkMax + 8 || nout > kBlkMax) return spm_fail(SPM_ERR_ARG, "combine size");
-  std::vector<double> buf((size_t)nin * nout + nout, 0.0);
-  std::copy(C.begin(), C.begin() + (size_t)nin * nout, buf.begin());
-  if (d) std::copy(d->begin(), d->begin() + nout, buf.begin() + (size_t)nin * nout);
-  // pageable source: the copy has consumed buf when the call returns
-  cudaError_t e = cudaMemcpyAsync(s->coef, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice,
-                                  c->stream);
-  if (e != cudaSuccess) return spm_fail_cuda(e, "combine coefficients");
   CombP p;
   std::memset(&p, 0, sizeof(p));
   for (int i = 0; i < nin; i++) p.X[i] = X[i];
@@ -136,9 +127,10 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
   p.nin = nin;
   p.nout = nout;
   p.n = npts(c);
-  p.C = s->coef;
-  p.d = d ? s->coef + (size_t)nin * nout : nullptr;
+  std::copy(C.begin(), C.begin() + (size_t)nin * nout, p.C);
+  if (d) std::copy(d->begin(), d->begin() + nout, p.d);
   p.accumulate = acc ? 1 : 0;
+  cudaError_t e = cudaSuccess;
   c->launches++;
   // register-bounded variants by block shape (two points per thread where they fit)
   auto launch = [&](auto kd, auto kf) {
@@ -383,7 +375,6 @@ void spm_free_extra(spm_ctx *c) {
   cudaFree(s->gram_part);
   cudaFree(s->gram_ticket);
   cudaFree(s->gram_out);
-  cudaFree(s->coef);
   cudaFree(s->lob);
   cudaFree(s->spm);
   cudaFree(s->spm_stats);
