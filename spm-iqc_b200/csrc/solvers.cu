@@ -99,10 +99,9 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
     else if (yt == 1) launch(gram_kernel<double, 4, 2, 1>, gram_kernel<float, 4, 2, 1>);
     else launch(gram_kernel<double, 4, 2>, gram_kernel<float, 4, 2>);
   } else {
-    // with Y aliased the B fragments take no registers of their own: four k-steps
-    if (yt == 0) launch(gram_kernel<double, 4, 3, 0>, gram_kernel<float, 4, 3, 0>);
-    else if (yt == 1) launch(gram_kernel<double, 4, 3, 1>, gram_kernel<float, 4, 3, 1>);
-    else if (yt == 2) launch(gram_kernel<double, 4, 3, 2>, gram_kernel<float, 4, 3, 2>);
+    if (yt == 0) launch(gram_kernel<double, 2, 3, 0>, gram_kernel<float, 2, 3, 0>);
+    else if (yt == 1) launch(gram_kernel<double, 2, 3, 1>, gram_kernel<float, 2, 3, 1>);
+    else if (yt == 2) launch(gram_kernel<double, 2, 3, 2>, gram_kernel<float, 2, 3, 2>);
     else launch(gram_kernel<double, 2, 3>, gram_kernel<float, 2, 3>);
   }
   cudaError_t e = cudaGetLastError();
