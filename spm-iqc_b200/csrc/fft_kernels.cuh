@@ -107,18 +107,6 @@ template <int N, class T, int RW = kRows, int R = 2> struct XgAreas {
   }
 };
 
-// Asks L2 for real-space row `row` (N values) of the auxiliary fields of
-// field b that a prologue or epilogue reads point by point (p.aux0, p.aux1).
-// (Rows are N * sizeof(T) >= 128 bytes, a multiple of 16; a field whose base
-// is not 16-byte aligned is not prefetched.)
-template <int N, class T> __device__ __forceinline__ void prefetch_aux_rows(const KParams &p, int b, size_t row) {
-  const void *a[2] = {p.aux0[b], p.aux1[b]};
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-    if (a[i] && ((uintptr_t)a[i] & 15u) == 0)
-      prefetch_l2(reinterpret_cast<const T *>(a[i]) + row * N, N * sizeof(T));
-}
-
 __device__ __forceinline__ void report_error(const KParams &p, int s_err) {
   if (s_err && p.err && threadIdx.x == 0) atomicExch(p.err, 1);
 }
@@ -505,9 +493,6 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
     // next plane's rows towards L2 while this one is transformed
     if (!STAGED && next < N && tid < RW)
       prefetch_l2(src + ((size_t)next * N + rank * RW + tid) * N, N * sizeof(T));
-    // and the rows of the fields the prologue reads beside it (phi of the
-    // Hessian product, the tangent fields of the force step, ...)
-    if (next < N && tid < RW) prefetch_aux_rows<N, T>(p, b, (size_t)next * N + rank * RW + tid);
     {
       const int j2 = tid & 7, r = tid >> 3;
       const size_t rowoff = ((size_t)plane * N + (size_t)(rank * RW + r)) * N;
@@ -866,8 +851,6 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_kernel(const __grid_con
     if (!STAGED && next < N)
       for (int i = tid; i < N; i += P::TH)
         prefetch_l2(gsrc + ((size_t)next * N + i) * M + rank * P::CW, P::CW * sizeof(T2));
-    // the next plane's rows of the fields the epilogue reads
-    if (next < N && tid < RW) prefetch_aux_rows<N, T>(p, b, (size_t)next * N + rank * RW + tid);
     P::template yi<(XG & kXgInv) != 0>(
         buf, tw, tid, cluster,
         [&](int ky, int c) -> T2 {
