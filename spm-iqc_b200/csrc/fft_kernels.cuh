@@ -44,33 +44,53 @@ template <int N, class T, int CPS, int RW = kRows> constexpr size_t plane_smem()
   return sizeof(c2<T>) * (N + N / 2 + RW * (N / 2) + (CPS == 1 ? Geo<N>::STAGE_UNITS : 0)) + 16 +
          sizeof(double) * 32 * kRedMax + 128;
 }
-// Pencil symbol table (per tile): 9 kz rows (the tile's 8 columns and kz = N/2)
-// x |Kx| = 0..N/2, one double2 half of the K^2 symbols each.
-template <int N> constexpr int pencil_sym_entries() { return 9 * (N / 2 + 1); }
-template <int N, class T> constexpr size_t pencil_smem_n(int stages, int symbufs) {
-  return sizeof(c2<T>) * (N + Geo<N>::PENCIL_UNITS + (size_t)stages * Geo<N>::STAGE_UNITS) + 16 +
-         sizeof(double) * 32 * kRedMax + sizeof(double2) * pencil_sym_entries<N>() * symbufs + 128;
+// Pencil tiles: the rows {ky, -ky} x TC spectral columns (TC = 8, or 4 for
+// the narrow variant), 2 TC x-pencils of N points, one CTA of 16 x 2 TC threads.
+template <int N, int TC = 8> struct PencilGeo {
+  static_assert(TC == 8 || TC == 4, "pencil tiles are 8 or 4 columns wide");
+  static constexpr int NP = 2 * TC;                   // pencils per tile
+  static constexpr int TH = 16 * NP;                  // threads per CTA
+  static constexpr int UNITS = Geo<N>::M1 * 16 * NP;  // x-transform exchange
+  static constexpr int STAGE = 2 * N * TC;            // one staged tile
+  static constexpr int NCH = (N / 2) / TC;            // column chunks per ky row
+  static constexpr int PTILES = (N / 2) * NCH;        // tiles per field
+  static constexpr int SYMN = (TC + 1) * (N / 2 + 1); // symbol entries per tile
+};
+// Pencil symbol table (per tile): TC + 1 kz rows (the tile's columns and
+// kz = N/2) x |Kx| = 0..N/2, one double2 half of the K^2 symbols each.
+template <int N, int TC = 8> constexpr int pencil_sym_entries() { return PencilGeo<N, TC>::SYMN; }
+template <int N, class T, int TC = 8> constexpr size_t pencil_smem_n(int stages, int symbufs) {
+  using PG = PencilGeo<N, TC>;
+  return sizeof(c2<T>) * (N + PG::UNITS + (size_t)stages * PG::STAGE) + 16 + sizeof(double) * 32 * kRedMax +
+         sizeof(double2) * PG::SYMN * symbufs + 128;
 }
 // CTAs of `smem` bytes that one SM holds (228 KB per SM, 1 KB reserved per CTA,
 // at most 227 KB per CTA).
 constexpr int smem_ctas_per_sm(size_t smem) { return smem > 232448 ? 0 : (int)(233472 / (smem + 1024)); }
 // Symbol buffers of the pencil: two (the next tile's copies start a whole
 // tile ahead) where the second one costs no resident CTA, else one.
-template <int N, class T> constexpr int pencil_sym_bufs(int stages, bool sym) {
+template <int N, class T, int TC = 8> constexpr int pencil_sym_bufs(int stages, bool sym) {
   return !sym ? 0
-         : smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 2)) == smem_ctas_per_sm(pencil_smem_n<N, T>(stages, 1)) ? 2
-                                                                                                               : 1;
+         : smem_ctas_per_sm(pencil_smem_n<N, T, TC>(stages, 2)) == smem_ctas_per_sm(pencil_smem_n<N, T, TC>(stages, 1))
+             ? 2
+             : 1;
 }
-// Resident pencil CTAs per SM the registers are budgeted for: two for FP32
-// pencils whose shared memory (one symbol buffer) lets two CTAs of 256
-// threads share an SM, which bounds them to 128 registers a thread; else one.
-// (At 256^3 FP32 the gradient pencil does not fit twice: one CTA with two
-// symbol buffers beat two CTAs with one buffer each.)
-template <int N, class T> constexpr int pencil_min_ctas(int stages, bool sym) {
-  return sizeof(T) == 4 && smem_ctas_per_sm(pencil_smem_n<N, T>(stages, sym ? 1 : 0)) >= 2 ? 2 : 1;
+// Resident pencil CTAs per SM the registers are budgeted for. 8-column tiles:
+// two for FP32 pencils whose shared memory (one symbol buffer) lets two CTAs
+// of 256 threads share an SM, which bounds them to 128 registers a thread;
+// else one. (At 256^3 FP32 the gradient pencil does not fit twice: one CTA
+// with two symbol buffers beat two CTAs with one buffer each.) 4-column tiles
+// (128 threads): as many as their shared memory allows, at most four.
+template <int N, class T, int TC = 8> constexpr int pencil_min_ctas(int stages, bool sym) {
+  if constexpr (TC == 4) {
+    const int k = smem_ctas_per_sm(pencil_smem_n<N, T, TC>(stages, pencil_sym_bufs<N, T, TC>(stages, sym)));
+    return k < 1 ? 1 : (k > 4 ? 4 : k);
+  } else {
+    return sizeof(T) == 4 && smem_ctas_per_sm(pencil_smem_n<N, T>(stages, sym ? 1 : 0)) >= 2 ? 2 : 1;
+  }
 }
-template <int N, class T> constexpr size_t pencil_smem(int stages, bool sym) {
-  return pencil_smem_n<N, T>(stages, pencil_sym_bufs<N, T>(stages, sym));
+template <int N, class T, int TC = 8> constexpr size_t pencil_smem(int stages, bool sym) {
+  return pencil_smem_n<N, T, TC>(stages, pencil_sym_bufs<N, T, TC>(stages, sym));
 }
 
 __device__ __forceinline__ unsigned char *smem_base128(unsigned char *raw) {
@@ -548,19 +568,22 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
 //       point in the full N^3 spectrum (1 on the kz = 0, N/2 planes, else 2).
 //     __device__ static void fin(const KParams&, int b, const double (&tot)[NR]);
 // Stages: [A (if FI)][S (if SI)], each 2 rows x N x 8 columns, [row][x][cc].
-template <int N, class T, class Op>
-__global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0))
+template <int N, class T, class Op, int TC = 8>
+__global__ void __launch_bounds__(PencilGeo<N, TC>::TH,
+                                  pencil_min_ctas<N, T, TC>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0))
     pencil_kernel(const __grid_constant__ KParams p) {
   using G = Geo<N>;
+  using PG = PencilGeo<N, TC>;
   using T2 = c2<T>;
   constexpr int M = G::M, M1 = G::M1;
+  constexpr int NP = PG::NP, TH = PG::TH, XU = 16 * NP;  // pencils, threads, exchange stride
   constexpr int NST = (Op::FI ? 1 : 0) + (Op::SI ? 1 : 0);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T2 *tw = reinterpret_cast<T2 *>(smem_base128(smem_raw));
   T2 *ex = tw + N;
-  T2 *sA = ex + G::PENCIL_UNITS;
-  T2 *sS = sA + (Op::FI ? G::STAGE_UNITS : 0);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(ex + G::PENCIL_UNITS + NST * G::STAGE_UNITS);
+  T2 *sA = ex + PG::UNITS;
+  T2 *sS = sA + (Op::FI ? PG::STAGE : 0);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ex + PG::UNITS + NST * PG::STAGE);
   double *red = reinterpret_cast<double *>(bars + 2);
   double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbol buffers (one or two tiles)
   __shared__ int s_err;
@@ -568,30 +591,30 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int b = blockIdx.y;
-  const int pen = tid & 15, rowsel = pen >> 3, cc = pen & 7;
+  const int pen = tid % NP, rowsel = pen / TC, cc = pen % TC;
   const uint64_t spol = l2_stream_policy();  // outputs: evict first
-  const bool has2 = (tid >> 4) < M1;  // owns a stage-2 task (pencil, k1)
-  const int k1 = tid >> 4;
+  const bool has2 = (tid / NP) < M1;  // owns a stage-2 task (pencil, k1)
+  const int k1 = tid / NP;
   // Tiles run columns-fastest, so concurrently resident CTAs read adjacent
-  // 8-column segments of the same ky rows.
-  constexpr int NCH = M / 8;
+  // TC-column segments of the same ky rows.
+  constexpr int NCH = PG::NCH;
   // Symbols: a tile's points have |Ky| = t (rows t and N - t, t > 0), Kz in
-  // its 8 columns (or N/2 for the packed c = 0 column) and any Kx, so the
-  // 9 x (N/2 + 1) entries it needs are staged in shared memory (the table
+  // its TC columns (or N/2 for the packed c = 0 column) and any Kx, so the
+  // (TC + 1) x (N/2 + 1) entries it needs are staged in shared memory (the table
   // lookups of every point would otherwise wait on L2). The copies are
   // asynchronous, awaited just before the tile's point operator; with two
   // buffers they start at the top of the previous tile, with one once the
   // previous tile's point operator is done. Tiles with t = 0 (rows 0 and
   // N/2) read the table.
   constexpr bool USE_SYM = Op::SYM >= 0;
-  constexpr int KXS = N / 2 + 1, SYMN = pencil_sym_entries<N>();
-  constexpr int SYMB = pencil_sym_bufs<N, T>(NST, USE_SYM);
+  constexpr int KXS = N / 2 + 1, SYMN = PG::SYMN;
+  constexpr int SYMB = pencil_sym_bufs<N, T, TC>(NST, USE_SYM);
   auto sym_stage = [&](int tl, double2 *dst) {
-    const int tt = tl / NCH, cz = (tl % NCH) * 8;
+    const int tt = tl / NCH, cz = (tl % NCH) * TC;
     const double2 *g = reinterpret_cast<const double2 *>(gtab_of(p, b)) + (USE_SYM ? Op::SYM : 0);
-    for (int e = tid; e < SYMN; e += kThreads) {
+    for (int e = tid; e < SYMN; e += TH) {
       const int row = e / KXS, a = e - row * KXS;
-      const int kz = row < 8 ? cz + row : N / 2;
+      const int kz = row < TC ? cz + row : N / 2;
       cp_async16(dst + e, g + 2 * (a * a + tt * tt + kz * kz));
     }
   };
@@ -602,13 +625,13 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
     else
       cp_async_wait_all();
   };
-  // thread 0: two tensor boxes (8 columns x all x) for rows ky0, ky1 of a tile
+  // thread 0: two tensor boxes (TC columns x all x) for rows ky0, ky1 of a tile
   auto issue = [&](const CUtensorMap *map, T2 *dst, uint64_t *bar, int tile) {
-    const int t = tile / NCH, c0 = (tile % NCH) * 8;
+    const int t = tile / NCH, c0 = (tile % NCH) * TC;
     const int ky0 = t, ky1 = (t == 0) ? N / 2 : N - t;
-    mbar_expect_tx(bar, (unsigned)(2 * N * 8 * sizeof(T2)));
+    mbar_expect_tx(bar, (unsigned)(2 * N * TC * sizeof(T2)));
     tma_load_3d(dst, map, 2 * c0, ky0, 0, bar);
-    tma_load_3d(dst + N * 8, map, 2 * c0, ky1, 0, bar);
+    tma_load_3d(dst + N * TC, map, 2 * c0, ky1, 0, bar);
   };
   if (tid == 0) {
     mbar_init(&bars[0], 1);
@@ -616,25 +639,25 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
     s_err = 0;
     fence_barrier_init();
   }
-  for (int i = tid; i < N; i += kThreads) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
+  for (int i = tid; i < N; i += TH) tw[i] = reinterpret_cast<const T2 *>(p.tw)[i];
   double acc[Op::NR > 0 ? Op::NR : 1];
 #pragma unroll
   for (int r = 0; r < (Op::NR > 0 ? Op::NR : 1); r++) acc[r] = ((Op::MAXM >> r) & 1u) ? -1.0e308 : 0.0;
   __syncthreads();
   int tile = blockIdx.x;
-  if (tid == 0 && tile < G::PTILES) {
+  if (tid == 0 && tile < PG::PTILES) {
     if (Op::FI) issue(&p.tmi[b], sA, &bars[0], tile);
     if (Op::SI) issue(&p.tms[b], sS, &bars[1], tile);
   }
   if constexpr (USE_SYM) {
-    if (tile < G::PTILES && tile / NCH != 0) sym_stage(tile, stab);
+    if (tile < PG::PTILES && tile / NCH != 0) sym_stage(tile, stab);
     if constexpr (SYMB == 2) cp_async_commit();
   }
 
-  for (int it = 0; tile < G::PTILES; tile += gridDim.x, it++) {
+  for (int it = 0; tile < PG::PTILES; tile += gridDim.x, it++) {
     const int next = tile + gridDim.x;
     const int t = tile / NCH;
-    const int c0 = (tile % NCH) * 8;
+    const int c0 = (tile % NCH) * TC;
     const int ky0 = t, ky1 = (t == 0) ? N / 2 : N - t;
     const int ky = rowsel ? ky1 : ky0;
     const int col = c0 + cc;
@@ -642,14 +665,14 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
     double2 *const sym_cur = stab + (SYMB == 2 ? (it & 1) * SYMN : 0);
     if constexpr (SYMB == 2) {
       // the other buffer's tile (two back) finished its point operator
-      if (next < G::PTILES && next / NCH != 0) sym_stage(next, stab + ((it + 1) & 1) * SYMN);
+      if (next < PG::PTILES && next / NCH != 0) sym_stage(next, stab + ((it + 1) & 1) * SYMN);
       cp_async_commit();
     }
     if constexpr (USE_SYM && !Op::FI) {
       sym_wait();
       __syncthreads();
     }
-    // symbols of (Kx, Ky, Kz) for kz row `row` of the tile (8: kz = N/2)
+    // symbols of (Kx, Ky, Kz) for kz row `row` of the tile (TC: kz = N/2)
     auto sym_at = [&](int Kx, int Ky, int Kz, int row) -> double2 {
       if constexpr (!USE_SYM) {
         return double2{0.0, 0.0};
@@ -662,28 +685,28 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
     T2 F[16];
     if constexpr (Op::FI) {
       mbar_wait(&bars[0], it & 1, &s_err);
-      {  // stage 1: task (pencil, j2 = tid/16): x = 16*j1 + j2
-        const int j2 = tid >> 4;
+      {  // stage 1: task (pencil, j2 = tid/NP): x = 16*j1 + j2
+        const int j2 = tid / NP;
         T2 v[M1];
         sfor<0, M1>([&](auto J1) {
           constexpr int j1 = SPM_CI(J1);
-          v[j1] = sA[(rowsel * N + 16 * j1 + j2) * 8 + cc];
+          v[j1] = sA[(rowsel * N + 16 * j1 + j2) * TC + cc];
         });
         Dft<-1, M1, T2>::run(v);
         sfor<0, M1>([&](auto K1) {
           constexpr int kk = SPM_CI(K1);
-          ex[kk * 256 + j2 * 16 + pen] = (kk == 0) ? v[kk] : cmul(v[kk], tw[j2 * kk]);
+          ex[kk * XU + j2 * NP + pen] = (kk == 0) ? v[kk] : cmul(v[kk], tw[j2 * kk]);
         });
       }
       if constexpr (USE_SYM) sym_wait();  // this tile's symbols, seen after the barrier
       __syncthreads();
-      if (tid == 0 && next < G::PTILES) {
+      if (tid == 0 && next < PG::PTILES) {
         fence_proxy_async();
         issue(&p.tmi[b], sA, &bars[0], next);
       }
       if (has2) {
 #pragma unroll
-        for (int j2 = 0; j2 < 16; j2++) F[j2] = ex[k1 * 256 + j2 * 16 + pen];
+        for (int j2 = 0; j2 < 16; j2++) F[j2] = ex[k1 * XU + j2 * NP + pen];
         Dft<-1, 16, T2>::run(F);  // F[k2] at kx = k1 + M1*k2
       }
     }
@@ -698,7 +721,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
           for (int k2 = 0; k2 < 16; k2++) {
             const int kx = k1 + M1 * k2;
             if constexpr (Op::FI) D[(0 * 2 + rowsel) * N + kx] = F[k2];
-            if constexpr (Op::SI) D[(1 * 2 + rowsel) * N + kx] = sS[(rowsel * N + kx) * 8];
+            if constexpr (Op::SI) D[(1 * 2 + rowsel) * N + kx] = sS[(rowsel * N + kx) * TC];
           }
         }
         __syncthreads();
@@ -714,7 +737,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
         const int kx = k1 + M1 * k2;
         const int Kx = wave(kx, N);
         const T2 f = Op::FI ? F[k2] : T2{0, 0};
-        const T2 s = Op::SI ? sS[(rowsel * N + kx) * 8 + cc] : T2{0, 0};
+        const T2 s = Op::SI ? sS[(rowsel * N + kx) * TC + cc] : T2{0, 0};
         T2 o_st = {0, 0}, o_inv = {0, 0};
         if (!Op::LIN && dc && cc == 0) {
           // unpack X(., ., 0) and X(., ., N/2), apply, repack
@@ -732,7 +755,7 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
           }
           T2 so0, inv0, soM, invM;
           Op::point(p, b, Kx, Ky, 0, sym_at(Kx, Ky, 0, 0), f0, s0, so0, inv0, acc, 1.0);
-          Op::point(p, b, Kx, Ky, -N / 2, sym_at(Kx, Ky, N / 2, 8), fM, sM, soM, invM, acc, 1.0);
+          Op::point(p, b, Kx, Ky, -N / 2, sym_at(Kx, Ky, N / 2, TC), fM, sM, soM, invM, acc, 1.0);
           o_st = T2{so0.x - soM.y, so0.y + soM.x};
           o_inv = T2{inv0.x - invM.y, inv0.y + invM.x};
         } else {
@@ -754,25 +777,25 @@ __global__ void __launch_bounds__(kThreads, pencil_min_ctas<N, T>((Op::FI ? 1 : 
     }
     __syncthreads();  // sS, stab and ex reads done
     if constexpr (Op::SI) {
-      if (tid == 0 && next < G::PTILES) {
+      if (tid == 0 && next < PG::PTILES) {
         fence_proxy_async();
         issue(&p.tms[b], sS, &bars[1], next);
       }
     }
     if constexpr (SYMB == 1)
-      if (next < G::PTILES && next / NCH != 0) sym_stage(next, stab);
+      if (next < PG::PTILES && next / NCH != 0) sym_stage(next, stab);
     if constexpr (Op::INV) {
       if (has2) {
         Dft<+1, 16, T2>::run(F);  // over k2 -> j2
 #pragma unroll
         for (int j2 = 0; j2 < 16; j2++)
-          ex[k1 * 256 + j2 * 16 + pen] = (j2 == 0 || k1 == 0) ? F[j2] : cmulc(F[j2], tw[j2 * k1]);
+          ex[k1 * XU + j2 * NP + pen] = (j2 == 0 || k1 == 0) ? F[j2] : cmulc(F[j2], tw[j2 * k1]);
       }
       __syncthreads();
       {
-        const int j2 = tid >> 4;
+        const int j2 = tid / NP;
         T2 v[M1];
-        sfor<0, M1>([&](auto K1) { v[SPM_CI(K1)] = ex[SPM_CI(K1) * 256 + j2 * 16 + pen]; });
+        sfor<0, M1>([&](auto K1) { v[SPM_CI(K1)] = ex[SPM_CI(K1) * XU + j2 * NP + pen]; });
         Dft<+1, M1, T2>::run(v);
         T2 *dst = reinterpret_cast<T2 *>(p.out[b]);
         sfor<0, M1>([&](auto J1) {

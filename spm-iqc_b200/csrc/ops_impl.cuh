@@ -216,15 +216,18 @@ template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx
   }
   return plane_inv_fwd_xg<N, T, Epi, Pro, 0>(c, p, nb);
 }
-// Persistent pencil launch: resident CTAs (queried once), at most one per tile.
-template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p0, int nb) {
+// Persistent pencil launch: resident CTAs (queried once), at most one per tile;
+// tiles of 8 columns, or 4 (knob "pencil_tc").
+template <int N, class T, class Op, int TC> static int pencil_tc(spm_ctx *c, const KParams &p0, int nb) {
+  using PG = PencilGeo<N, TC>;
   KParams p = p0;
+  const int kind = TC == 8 ? TM_PENCIL : TM_PENCIL4;
   for (int b = 0; b < nb; b++) {
-    if (Op::FI) SPM_TRY(spm_tensor_map(c, p.in[b], TM_PENCIL, &p.tmi[b]));
-    if (Op::SI) SPM_TRY(spm_tensor_map(c, p.st[b], TM_PENCIL, &p.tms[b]));
+    if (Op::FI) SPM_TRY(spm_tensor_map(c, p.in[b], kind, &p.tmi[b]));
+    if (Op::SI) SPM_TRY(spm_tensor_map(c, p.st[b], kind, &p.tms[b]));
   }
-  auto kern = pencil_kernel<N, T, Op>;
-  constexpr size_t smem = pencil_smem<N, T>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0);
+  auto kern = pencil_kernel<N, T, Op, TC>;
+  constexpr size_t smem = pencil_smem<N, T, TC>((Op::FI ? 1 : 0) + (Op::SI ? 1 : 0), Op::SYM >= 0);
   static_assert(smem_ctas_per_sm(smem) >= 1, "pencil shared memory above the 227 KB a CTA may use");
   struct Tag {};
   cudaError_t e = prepare<Tag>(kern, smem, c->device);
@@ -234,17 +237,21 @@ template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams 
   int nbk = nblk[dev].load(std::memory_order_relaxed);
   if (nbk == 0) {
     int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PG::TH, smem);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     if (e != cudaSuccess || per_sm < 1) return spm_fail_cuda(e != cudaSuccess ? e : cudaErrorInvalidConfiguration,
                                                              "pencil occupancy");
-    nbk = per_sm * sms < Geo<N>::PTILES ? per_sm * sms : Geo<N>::PTILES;
+    nbk = per_sm * sms < PG::PTILES ? per_sm * sms : PG::PTILES;
     nblk[dev].store(nbk, std::memory_order_relaxed);
   }
   c->launches++;
-  kern<<<dim3(nbk, nb, 1), kThreads, smem, c->stream>>>(p);
+  kern<<<dim3(nbk, nb, 1), PG::TH, smem, c->stream>>>(p);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, "pencil launch");
+}
+template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p, int nb) {
+  if (c->pencil_tc == 4) return pencil_tc<N, T, Op, 4>(c, p, nb);
+  return pencil_tc<N, T, Op, 8>(c, p, nb);
 }
 template <int N, class T, class F> static int reduce(spm_ctx *c, const KParams &p, int nb) {
   constexpr size_t npairs = (size_t)N * N * N / 2;

@@ -167,8 +167,8 @@ int spm_tensor_map(spm_ctx *c, const void *ptr, int kind, CUtensorMap *out) {
   const cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)N};  // N reals = N/2 complex per row
   const cuuint64_t strides[2] = {(cuuint64_t)N * es, (cuuint64_t)N * N * es};
   cuuint32_t box[3];
-  if (kind == TM_PENCIL) {
-    box[0] = 16;  // 8 complex columns
+  if (kind == TM_PENCIL || kind == TM_PENCIL4) {
+    box[0] = kind == TM_PENCIL ? 16 : 8;  // 8 or 4 complex columns
     box[1] = 1;
     box[2] = (cuuint32_t)N;
   } else {
@@ -384,6 +384,11 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->batch_group = value;
     return SPM_OK;
   }
+  if (std::strcmp(knob, "pencil_tc") == 0) {
+    if (value != 8 && value != 4) return spm_fail(SPM_ERR_ARG, "pencil_tc must be 8 or 4");
+    c->pencil_tc = value;
+    return SPM_OK;
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
@@ -393,6 +398,7 @@ extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (std::strcmp(knob, "fuse_planes") == 0) return c->fuse_planes;
   if (std::strcmp(knob, "plane_xg") == 0) return c->plane_xg;
   if (std::strcmp(knob, "batch_group") == 0) return c->batch_group;
+  if (std::strcmp(knob, "pencil_tc") == 0) return c->pencil_tc;
   return -1;
 }
 
@@ -583,6 +589,7 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->fuse_planes = c->fuse_planes;
   c->twin->plane_xg = c->plane_xg;
   c->twin->batch_group = c->batch_group;
+  c->twin->pencil_tc = c->pencil_tc;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
   spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg);
   return spm_ensure_xg(c->twin);

@@ -12,8 +12,9 @@
 
 // Box shapes of the tensor copies over a packed spectrum [x][ky][2*(N/2) reals].
 enum TmKind {
-  TM_PENCIL = 0,    // 8 complex columns x 1 ky row x all N x
-  TM_PLANE_INV = 1  // 16 complex columns x all N ky x 1 x-plane
+  TM_PENCIL = 0,     // 8 complex columns x 1 ky row x all N x
+  TM_PLANE_INV = 1,  // 16 complex columns x all N ky x 1 x-plane
+  TM_PENCIL4 = 2     // 4 complex columns x 1 ky row x all N x (narrow pencil tiles)
 };
 struct TmEntry {
   const void *ptr;
@@ -54,6 +55,7 @@ struct spm_ctx {
   void *xg = nullptr;           // their global exchange areas (2 x xg_cap CTAs x 16 N complex)
   int xg_cap = 0;
   int batch_group = 1;          // spm_batch_grad_flow: same-size instances share launches (knob "batch_group")
+  int pencil_tc = 8;            // pencil tile width in complex columns: 8 or 4 (knob "pencil_tc")
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
   const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)

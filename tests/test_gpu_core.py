@@ -188,3 +188,31 @@ def test_autotune_picks_a_schedule_and_keeps_results(spm, cuda):
     for st, p in out[1:]:
         assert np.array_equal(p, out[0][1])
         assert rel(st, out[0][0]) < 1e-13
+
+
+@pytest.mark.parametrize("N,prec", [(32, "fp64"), (64, "fp64"), (256, "fp64"), (96, "fp32"), (256, "fp32")])
+def test_narrow_pencil_tiles_are_bit_identical(spm, cuda, N, prec):
+    """Pencil passes with 4-column tiles (knob pencil_tc 4: 8 pencils and 128
+    threads per CTA, several CTAs per SM) give the same fields as 8-column
+    tiles, for gradient steps, a Hessian-vector block and the preconditioner;
+    reductions (step records) agree to rounding (their summation order
+    follows the tiling)."""
+    phi = npo.uniform_field(N, 19)
+    V = np.stack([npo.uniform_field(N, 50 + i, amp=1.0) for i in range(2)])
+    dt = np.float64 if prec == "fp64" else np.float32
+    out = []
+    for tc in (8, 4):
+        e = spm.SpmContext(N, Tau=-0.02, precision=prec)
+        e.tune("pencil_tc", tc)
+        p = t(cuda, phi.astype(dt))
+        u = e.my_fft(p)
+        st = e.get_min_u_F(p, u, 17)
+        H = e.hv_cam(p, t(cuda, V.astype(dt)))
+        W = t(cuda, V.astype(dt))
+        e.precond_camnew(W)
+        out.append((st, p.cpu().numpy(), u.cpu().numpy(), H.cpu().numpy(), W.cpu().numpy()))
+        e.close()
+    (s8, p8, u8, h8, w8), (s4, p4, u4, h4, w4) = out
+    assert np.array_equal(p8, p4) and np.array_equal(u8, u4)
+    assert np.array_equal(h8, h4) and np.array_equal(w8, w4)
+    assert rel(s4, s8) < (1e-12 if prec == "fp64" else 1e-5)
