@@ -99,14 +99,20 @@ const char *spm_status_str(int status);
  * stay resident in L2 (bit 1: the forward exchange, bit 2: the inverse one;
  * the same bits either way). Nonzero allocates the areas (4 x resident CTAs x
  * 16 N complex values).
+ * knob "pencil_tc" (8 or 4): the width in spectral columns of the pencil
+ * passes' tiles; 4 halves a CTA's shared memory and threads so that several
+ * CTAs share an SM (the same bits either way).
+ * knob "batch_group" (1 or 0): spm_batch_grad_flow lets instances of the same
+ * N and precision share every launch (1) or gives each its own (0).
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);
 /* Autotuner (no counterpart in the reference): times chains of `steps`
  * gradient steps on a scratch field for each candidate schedule (plane_cps
  * 1/2/3 with fused chains, plane_cps 2 without, plane_xg 1/2/3 with plane_cps
- * 2 and 3 on fused chains, plane_cps 4 for FP32, 5, 6) and keeps the fastest in the
- * context; the choice is remembered per (device, N, precision), so later
+ * 2 and 3 on fused chains, plane_cps 4 for FP32, 5, 6; then pencil_tc 4 for the
+ * best of them), keeping a later candidate only if it is at least 1 % faster, and
+ * keeps the fastest in the context; the choice is remembered per (device, N, precision), so later
  * contexts of the same kind take it without timing (FP32 twins of mixed flows
  * included). Synchronises; allocates two scratch fields while it runs. The
  * chosen knobs are returned in *plane_cps, *fuse_planes (may be NULL);

@@ -22,7 +22,7 @@ namespace {
 
 std::mutex g_mu;
 struct Choice {
-  int plane_cps, fuse_planes, plane_xg;
+  int plane_cps, fuse_planes, plane_xg, pencil_tc = 8;
 };
 std::map<std::tuple<int, int, int>, Choice> g_best;  // (device, N, prec) -> schedule
 
@@ -40,13 +40,15 @@ template <class T> __global__ void fill_kernel(T *phi, int N) {
 }  // namespace
 
 // The remembered choice for (device, N, precision), if any.
-bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg) {
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg,
+                         int *pencil_tc) {
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_best.find(std::make_tuple(device, N, prec));
   if (it == g_best.end()) return false;
   *plane_cps = it->second.plane_cps;
   *fuse_planes = it->second.fuse_planes;
   *plane_xg = it->second.plane_xg;
+  if (pencil_tc) *pencil_tc = it->second.pencil_tc;
   return true;
 }
 
@@ -57,6 +59,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
     c->plane_cps = ch.plane_cps;
     c->fuse_planes = ch.fuse_planes;
     c->plane_xg = ch.plane_xg;
+    c->pencil_tc = ch.pencil_tc;
     if (!c->plane_xg && c->xg) {  // the exchange areas are not used by the chosen schedule
       cudaStreamSynchronize(c->stream);
       cudaFree(c->xg);
@@ -82,7 +85,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   int rc = e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "autotune buffers");
-  const Choice saved = {c->plane_cps, c->fuse_planes, c->plane_xg};
+  const Choice saved = {c->plane_cps, c->fuse_planes, c->plane_xg, c->pencil_tc};
   Choice best = saved;
   float best_ms = 1e30f;
   // plane variant, fused plane pass, exchange routes of the gradient chains
@@ -92,33 +95,52 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   if (c->prec == SPM_FP32) all.push_back({4, 1, spm::kXgFwd | spm::kXgInv});  // four CTAs per SM
   all.push_back({5, 1, spm::kXgFwd | spm::kXgInv});  // 16-row CTAs, four per SM
   all.push_back({6, 1, spm::kXgFwd | spm::kXgInv});  // the same, fused pass pipelined over planes
-  for (const Choice &cand : all) {
-    if (rc != SPM_OK) break;
+  // best of three timed chains of `steps` gated steps with the candidate's knobs
+  auto time_it = [&](const Choice &cand, float &t) -> int {
     c->plane_cps = cand.plane_cps;
     c->fuse_planes = cand.fuse_planes;
     c->plane_xg = cand.plane_xg;
-    rc = spm_ensure_xg(c);
-    if (rc != SPM_OK) break;
+    c->pencil_tc = cand.pencil_tc;
+    int r = spm_ensure_xg(c);
+    if (r != SPM_OK) return r;
     if (c->prec == SPM_FP64) fill_kernel<double><<<592, 256, 0, c->stream>>>((double *)phi, c->N);
     else fill_kernel<float><<<592, 256, 0, c->stream>>>((float *)phi, c->N);
-    rc = spm_fft(c, phi, uh);
+    r = spm_fft(c, phi, uh);
     // warm-up (kernel attributes, occupancy queries, caches), then the best of three timed chains
-    if (rc == SPM_OK) rc = spm_grad_flow_enqueue(c, phi, uh, 3, 0.0);
-    if (rc == SPM_OK) rc = spm_grad_flow_collect(c, nullptr, 0, nullptr);
-    float t = 1e30f;
-    for (int r = 0; r < 3 && rc == SPM_OK; r++) {
+    if (r == SPM_OK) r = spm_grad_flow_enqueue(c, phi, uh, 3, 0.0);
+    if (r == SPM_OK) r = spm_grad_flow_collect(c, nullptr, 0, nullptr);
+    t = 1e30f;
+    for (int rep = 0; rep < 3 && r == SPM_OK; rep++) {
       cudaEventRecord(e0, c->stream);
-      rc = spm_grad_flow_enqueue(c, phi, uh, steps, 0.0);
+      r = spm_grad_flow_enqueue(c, phi, uh, steps, 0.0);
       cudaEventRecord(e1, c->stream);
-      if (rc == SPM_OK) rc = spm_grad_flow_collect(c, nullptr, 0, nullptr);
+      if (r == SPM_OK) r = spm_grad_flow_collect(c, nullptr, 0, nullptr);
       float ms = 0;
-      if (rc == SPM_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < t) t = ms;
+      if (r == SPM_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < t) t = ms;
     }
+    return r;
+  };
+  for (const Choice &cand : all) {
+    if (rc != SPM_OK) break;
+    float t = 1e30f;
+    rc = time_it(cand, t);
     // a later candidate must be at least 1 % faster to replace the best so far
     // (candidates within timing noise of each other resolve to the earlier one)
     if (rc == SPM_OK && t < 0.99f * best_ms) {
       best_ms = t;
       best = cand;
+    }
+  }
+  // then the pencil tile width for the best schedule: 4-column tiles (several
+  // CTAs per SM) if they are at least 1 % faster
+  if (rc == SPM_OK) {
+    Choice narrow = best;
+    narrow.pencil_tc = 4;
+    float t = 1e30f;
+    rc = time_it(narrow, t);
+    if (rc == SPM_OK && t < 0.99f * best_ms) {
+      best_ms = t;
+      best = narrow;
     }
   }
   if (e0) cudaEventDestroy(e0);

@@ -92,5 +92,6 @@ struct FloorWatch {
 };
 
 // The autotuner's remembered choice for (device, N, precision), if any.
-bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg);
+bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg,
+                         int *pencil_tc = nullptr);
 const struct OpsTable *spm_table_of(const spm_ctx *c);
