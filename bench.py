@@ -304,7 +304,9 @@ def reference_arm(args, rank, world):
 
 # Step caps of the serving jobs: each job runs to ||grad F|| (LOBPCG: the
 # block residual) <= 1e-8 and stops there; the cap only bounds jobs whose
-# stationary point keeps the flow above the tolerance.
+# stationary point keeps the flow above the tolerance (a saddle, or a minimum
+# whose rounding floor of ||grad F|| lies near 1e-8, as the SPM saddle search's
+# index-1 point at 256^3 does with a floor of about 1.08e-8).
 SERVE_CAPS = {"relax": 20000, "lobpcg": 400, "spm": 3000}
 
 
