@@ -277,6 +277,24 @@ int spm_gosd(spm_ctx *ctx, void *x, void *V, int k, const void *V0, int k0, doub
 /* inpfp (BasicOperators.cpp:132-143): <p, q> = (1/N^3) sum p q. */
 int spm_inpfp(spm_ctx *ctx, const void *p, const void *q, double *out);
 
+/* Block of inner products, the Gram of LOBPCG.cpp:336-358 (UUm * YYm^T /
+ * N^3): G[a*mb + b] = <X[a], Y[b]> for a < ma, b < mb (1 <= ma, mb <= 24;
+ * X and Y are host arrays of device field pointers, which may repeat fields
+ * or share them between X and Y; each distinct field is read once), G a host
+ * array of ma*mb doubles. Runs on the FP64 tensor cores; the sums are in a
+ * fixed order (identical results on every call). Synchronises the context's
+ * stream. */
+int spm_block_gram(spm_ctx *ctx, const void *const *X, int ma, const void *const *Y, int mb, double *G);
+
+/* Block combination, the Ritz-vector update of LOBPCG.cpp:403-418 (Vm =
+ * eta1^T UUm): Y[q] = sum_p C[p*nout + q] X[p] + d[q] for q < nout (1 <= nin
+ * <= 32, 1 <= nout <= 24; X, Y host arrays of device field pointers; C a host
+ * array of nin*nout doubles, d of nout doubles or NULL for zeros). A point's
+ * inputs are all read before any of its outputs is written, so Y may alias X
+ * (an in-place update). Enqueued on the context's stream. */
+int spm_block_combine(spm_ctx *ctx, const void *const *X, int nin, void *const *Y, int nout, const double *C,
+                      const double *d);
+
 /* Allocation-free batch of inner products; no counterpart in the reference.
  * For callers that cannot allocate device memory when they need the result
  * (their device memory is fully reserved by their own pool, or a cudaMalloc's

@@ -11,6 +11,9 @@ constexpr int kBlkMax = 24;      // vectors per block operand (3k with k <= 8)
 constexpr int kGramBlocks = 296; // 2 CTAs per SM
 constexpr int kGramWarps = 8;
 
+constexpr int kStageBlocks = 148;  // staged Gram: one CTA per SM of a B200 (a fixed grid: fixed partial sums)
+constexpr int kStageWarps = 16;    // its consumer warps (plus one producer warp)
+
 struct GramP {
   const void *X[kBlkMax];
   const void *Y[kBlkMax];
@@ -19,8 +22,15 @@ struct GramP {
   double inv_n;      // normalisation of <.,.> (1/N^3)
   double *partials;  // [kGramBlocks][kBlkMax * kBlkMax]
   unsigned *ticket;
-  double *out;       // ma x mb, row-major
+  double *out;       // ma x mb, row-major (the staged kernel adds out[ma*mb]: its error flag)
   const int *flow;   // optional gate
+  // staged kernel only: the distinct fields of X and Y, each staged once
+  const void *F[2 * kBlkMax];
+  unsigned char xf[kBlkMax], yf[kBlkMax];  // X_a = F[xf[a]], Y_b = F[yf[b]]
+  int nf;
+  int chunk_bytes;   // bytes of one field per chunk (a multiple of 128 dividing the field)
+  int stages;
+  int *err;          // the context's error word (bounded waits)
 };
 
 __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
@@ -137,6 +147,163 @@ __global__ void __launch_bounds__(kGramWarps * 32) gram_kernel(const __grid_cons
   if (threadIdx.x == 0) *p.ticket = 0u;
 }
 
+// The same Gram with the fields staged through shared memory. Each CTA streams
+// its chunks (chunk c: points [c CH, (c+1) CH) of every distinct field, CH =
+// chunk_bytes / sizeof(T); CTA b takes chunks b, b + grid, ...) through a ring
+// of `stages` buffers. A producer warp issues one bulk copy per field and
+// chunk (lane f copies field f), completing on the buffer's "full" mbarrier,
+// and refills a buffer once the 16 consumer warps have arrived on its "empty"
+// mbarrier, so the consumers never wait for one another and a whole chunk of
+// every field is in flight per buffer without registers or per-thread loads.
+// The consumers read the fragments from shared memory (rows padded by 16
+// bytes: the 8 rows x 4 lanes of a fragment load fall in distinct bank
+// groups) and issue the same DMMA m8n8k4 pairs as gram_kernel. A field that
+// is both an X and a Y operand (the aliased Grams of the block
+// orthogonalisations) is read from HBM once. Sums are in a fixed order: a
+// warp's k-steps in chunk order, then the warps, then the CTAs.
+// TA / TB: 8-vector tiles of X / Y (ma <= 8 TA, mb <= 8 TB).
+template <class T, int TA, int TB>
+__global__ void __launch_bounds__((kStageWarps + 1) * 32, 1) gram_staged_kernel(const __grid_constant__ GramP p) {
+  constexpr int NW = kStageWarps + 1;  // warps: consumers 0..15, producer 16
+  extern __shared__ __align__(128) unsigned char gsm_raw[];
+  __shared__ int s_err, s_last, s_issued;
+  if (p.flow && *((volatile const int *)p.flow) == 0) return;
+  unsigned char *st = smem_base128(gsm_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int nf = p.nf, CB = p.chunk_bytes, RS = CB + 16, ST = p.stages;
+  const int CH = CB / (int)sizeof(T);
+  uint64_t *full = reinterpret_cast<uint64_t *>(st + (size_t)ST * nf * RS);
+  uint64_t *empty = full + ST;
+  using V2 = c2<T>;
+  const size_t nch = p.n / (size_t)CH;
+  const int mine = nch > blockIdx.x ? (int)((nch - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  if (tid == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kStageWarps);
+    }
+    s_err = 0;
+    s_issued = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  double acc[TA][TB][2];
+#pragma unroll
+  for (int i = 0; i < TA; i++)
+#pragma unroll
+    for (int j = 0; j < TB; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (warp == kStageWarps) {
+    // producer: chunk i into buffer i % ST once chunk i - ST is consumed
+    for (int i = 0; i < mine; i++) {
+      const int s = i % ST;
+      const bool ok = i < ST || mbar_wait(&empty[s], (unsigned)((i / ST - 1) & 1), &s_err);
+      if (!__all_sync(0xffffffffu, ok)) break;  // the warp leaves together
+      const size_t c = blockIdx.x + (size_t)i * gridDim.x;
+      if (lane == 0) mbar_expect_tx(&full[s], (unsigned)(nf * CB));
+      __syncwarp();
+      unsigned char *dst = st + (size_t)s * nf * RS;
+      for (int f = lane; f < nf; f += 32)
+        bulk_g2s(dst + (size_t)f * RS, reinterpret_cast<const unsigned char *>(p.F[f]) + c * CB, (unsigned)CB,
+                 &full[s]);
+      if (lane == 0) s_issued = i + 1;
+    }
+  } else {
+    // this lane's fragment rows (byte offsets within a buffer; -1: beyond ma / mb)
+    int ra[TA], rb[TB];
+#pragma unroll
+    for (int t = 0; t < TA; t++) ra[t] = (8 * t + gid < p.ma) ? (int)p.xf[8 * t + gid] * RS : -1;
+#pragma unroll
+    for (int t = 0; t < TB; t++) rb[t] = (8 * t + gid < p.mb) ? (int)p.yf[8 * t + gid] * RS : -1;
+    for (int i = 0; i < mine; i++) {
+      const int s = i % ST;
+      const bool ok = mbar_wait(&full[s], (unsigned)((i / ST) & 1), &s_err);
+      if (!__all_sync(0xffffffffu, ok)) break;  // the warp leaves together
+      const unsigned char *buf = st + (size_t)s * nf * RS;
+      // 8-point groups g of the chunk: lane (gid, tig) takes points 8g + 2 tig, +1
+      for (int g = warp; g < CH / 8; g += kStageWarps) {
+        V2 a[TA], b[TB];
+#pragma unroll
+        for (int t = 0; t < TA; t++)
+          a[t] = ra[t] >= 0 ? reinterpret_cast<const V2 *>(buf + ra[t])[4 * g + tig] : V2{0, 0};
+#pragma unroll
+        for (int t = 0; t < TB; t++)
+          b[t] = rb[t] >= 0 ? reinterpret_cast<const V2 *>(buf + rb[t])[4 * g + tig] : V2{0, 0};
+#pragma unroll
+        for (int ii = 0; ii < TA; ii++)
+#pragma unroll
+          for (int j = 0; j < TB; j++) {
+            dmma_8x8x4(acc[ii][j][0], acc[ii][j][1], (double)a[ii].x, (double)b[j].x);
+            dmma_8x8x4(acc[ii][j][0], acc[ii][j][1], (double)a[ii].y, (double)b[j].y);
+          }
+      }
+      // this warp is done reading buffer s: order its reads before the
+      // producer's next bulk copy into it
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (s_err) {
+      // a wait gave up: let the copies still in flight land (bounded) before
+      // the buffers are reused below or the CTA exits
+      const int issued = s_issued;
+      for (int i = issued > ST ? issued - ST : 0; i < issued; i++)
+        for (long k = 0; k < kSpinLimit && !mbar_try_wait(&full[i % ST], (unsigned)((i / ST) & 1)); k++)
+          __nanosleep(256);
+    }
+    for (int s = 0; s < ST; s++) {
+      mbar_inval(&full[s]);
+      mbar_inval(&empty[s]);
+    }
+  }
+  __syncthreads();
+  // CTA total in a fixed warp order (the ring's bytes hold the per-warp tiles)
+  double *tile = reinterpret_cast<double *>(st);
+  constexpr int RA = 8 * TA, RB = 8 * TB;
+  if (warp < kStageWarps) {
+#pragma unroll
+    for (int i = 0; i < TA; i++)
+#pragma unroll
+      for (int j = 0; j < TB; j++) {
+        const int r = i * 8 + gid, c = j * 8 + 2 * tig;
+        tile[(warp * RA + r) * RB + c] = acc[i][j][0];
+        tile[(warp * RA + r) * RB + c + 1] = acc[i][j][1];
+      }
+  }
+  __syncthreads();
+  double *part = p.partials + (size_t)blockIdx.x * kBlkMax * kBlkMax;
+  for (int e = tid; e < RA * RB; e += NW * 32) {
+    double s = 0.0;
+    for (int w = 0; w < kStageWarps; w++) s += tile[w * RA * RB + e];
+    part[(e / RB) * kBlkMax + e % RB] = s;
+  }
+  if (tid == 0 && s_err) atomicExch(p.err, 1);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(p.ticket, 1u) == gridDim.x - 1u);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // grid total of every entry in a fixed order (as gram_kernel)
+  for (int e = warp; e < p.ma * p.mb; e += NW) {
+    const int r = e / p.mb, c = e % p.mb;
+    double s = 0.0;
+#pragma unroll 4
+    for (unsigned bk = lane; bk < gridDim.x; bk += 32)
+      s += __ldcg(p.partials + (size_t)bk * kBlkMax * kBlkMax + r * kBlkMax + c);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) p.out[e] = s * p.inv_n;
+  }
+  if (tid == 0) {
+    p.out[p.ma * p.mb] = (double)*((volatile int *)p.err);
+    *p.ticket = 0u;
+  }
+}
+
 // The coefficients travel in the kernel parameters (6.3 KB), so a
 // combination needs no host-to-device copy (and no stream synchronisation
 // for one) before its launch.
@@ -149,6 +316,14 @@ struct CombP {
   double d[kBlkMax];                  // nout constants (zeros when none)
   int accumulate;                     // Y_q = (accumulate ? Y_q : 0) + ...
   const int *flow;
+  // staged kernel only (no accumulation; C packed with row stride kBlkMax:
+  // C[p * kBlkMax + q]): the distinct inputs, each staged once
+  const void *F[kBlkMax + 8];
+  unsigned char xf[kBlkMax + 8];      // X_p = F[xf[p]]
+  int nf;
+  int chunk_bytes;                    // as GramP
+  int stages;
+  int *err;
 };
 
 // Y_q[i] = (accumulate ? Y_q[i] : 0) + sum_p C[p][q] X_p[i] + d[q]. A point's
@@ -214,6 +389,101 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
         }
         Pts<T, PTS>::st(p.Y[q], i, o);
       }
+    }
+  }
+}
+
+// The same combination (without accumulation, nout <= NO) with the inputs
+// staged through shared memory by a producer warp, as gram_staged_kernel
+// does: chunk c of every distinct input lands in a ring buffer, and one of two
+// groups of 8 consumer warps (alternate chunks, so two chunks are worked on at
+// once) computes the chunk's outputs point by point (thread j of the
+// chunk: Y_q[j] = sum_p C[p][q] X_p[j] + d[q], the coefficients read from the
+// kernel parameters at fixed offsets) and store them. Same operations in the
+// same order as combine_kernel, so the results are the same bits. A chunk's
+// inputs are all in shared memory before any of its outputs is stored, and
+// chunks are disjoint, so Y may alias X.
+constexpr int kCombWarps = 16;  // consumer warps: two groups of 8, taking alternate chunks
+constexpr int kCombGroupWarps = 8;
+template <class T, int NI, int NO>
+__global__ void __launch_bounds__((kCombWarps + 1) * 32, 1) combine_staged_kernel(const __grid_constant__ CombP p) {
+  extern __shared__ __align__(128) unsigned char csm_raw[];
+  __shared__ int s_err, s_issued;
+  if (p.flow && *((volatile const int *)p.flow) == 0) return;
+  unsigned char *st = smem_base128(csm_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nf = p.nf, CB = p.chunk_bytes, RS = CB + 16, ST = p.stages;
+  const int CH = CB / (int)sizeof(T);
+  uint64_t *full = reinterpret_cast<uint64_t *>(st + (size_t)ST * nf * RS);
+  uint64_t *empty = full + ST;
+  const size_t nch = p.n / (size_t)CH;
+  const int mine = nch > blockIdx.x ? (int)((nch - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  if (tid == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kCombGroupWarps);
+    }
+    s_err = 0;
+    s_issued = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (warp == kCombWarps) {
+    for (int i = 0; i < mine; i++) {
+      const int s = i % ST;
+      const bool ok = i < ST || mbar_wait(&empty[s], (unsigned)((i / ST - 1) & 1), &s_err);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      const size_t c = blockIdx.x + (size_t)i * gridDim.x;
+      if (lane == 0) mbar_expect_tx(&full[s], (unsigned)(nf * CB));
+      __syncwarp();
+      unsigned char *dst = st + (size_t)s * nf * RS;
+      for (int f = lane; f < nf; f += 32)
+        bulk_g2s(dst + (size_t)f * RS, reinterpret_cast<const unsigned char *>(p.F[f]) + c * CB, (unsigned)CB,
+                 &full[s]);
+      if (lane == 0) s_issued = i + 1;
+    }
+  } else {
+    const int grp = warp / kCombGroupWarps, gt = tid - grp * kCombGroupWarps * 32;
+    for (int i = grp; i < mine; i += kCombWarps / kCombGroupWarps) {
+      const int s = i % ST;
+      const bool ok = mbar_wait(&full[s], (unsigned)((i / ST) & 1), &s_err);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      const unsigned char *buf = st + (size_t)s * nf * RS;
+      const size_t base = (blockIdx.x + (size_t)i * gridDim.x) * (size_t)CH;
+      for (int j = gt; j < CH; j += kCombGroupWarps * 32) {
+        double o[NO];
+#pragma unroll
+        for (int q = 0; q < NO; q++) o[q] = 0.0;
+#pragma unroll
+        for (int r = 0; r < NI; r++) {
+          if (r < p.nin) {
+            const double x = (double)reinterpret_cast<const T *>(buf + (size_t)p.xf[r] * RS)[j];
+#pragma unroll
+            for (int q = 0; q < NO; q++) o[q] = __fma_rn(p.C[r * kBlkMax + q], x, o[q]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NO; q++)
+          if (q < p.nout) reinterpret_cast<T *>(p.Y[q])[base + j] = (T)(o[q] + p.d[q]);
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (s_err) {
+      // a wait gave up: let the copies still in flight land (bounded)
+      const int issued = s_issued;
+      for (int i = issued > ST ? issued - ST : 0; i < issued; i++)
+        for (long k = 0; k < kSpinLimit && !mbar_try_wait(&full[i % ST], (unsigned)((i / ST) & 1)); k++)
+          __nanosleep(256);
+      atomicExch(p.err, 1);
+    }
+    for (int s = 0; s < ST; s++) {
+      mbar_inval(&full[s]);
+      mbar_inval(&empty[s]);
     }
   }
 }

@@ -53,8 +53,8 @@ int ensure_base(spm_ctx *c) {
   cudaError_t e = cudaMalloc(&s->gram_part, sizeof(double) * kGramBlocks * kBlkMax * kBlkMax);
   if (e == cudaSuccess) e = cudaMalloc(&s->gram_ticket, sizeof(unsigned) * 4);
   if (e == cudaSuccess) e = cudaMemset(s->gram_ticket, 0, sizeof(unsigned) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&s->gram_out, sizeof(double) * kBlkMax * kBlkMax);
-  if (e == cudaSuccess) e = cudaMallocHost(&s->h_gram, sizeof(double) * kBlkMax * kBlkMax);
+  if (e == cudaSuccess) e = cudaMalloc(&s->gram_out, sizeof(double) * (kBlkMax * kBlkMax + 8));
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_gram, sizeof(double) * (kBlkMax * kBlkMax + 8));
   if (e != cudaSuccess) return spm_fail_cuda(e, "solver buffers");
   return SPM_OK;
 }
@@ -62,8 +62,67 @@ int ensure_base(spm_ctx *c) {
 inline size_t npts(const spm_ctx *c) { return (size_t)c->N * c->N * c->N; }
 inline void *fld(const spm_ctx *c, void *base, int i) { return (char *)base + c->field_bytes * (size_t)i; }
 
+// Shared memory of the staged Gram: the stage ring, its mbarriers, and (after
+// the loop, over the same bytes) the per-warp tiles of the CTA total.
+static size_t gram_staged_smem(const GramP &p) {
+  const size_t ring = (size_t)p.stages * p.nf * (p.chunk_bytes + 16) + 16 * (size_t)p.stages;
+  const size_t tiles = sizeof(double) * kStageWarps * (size_t)(8 * ((p.ma + 7) / 8)) * (8 * ((p.mb + 7) / 8));
+  return std::max(ring, tiles) + 128;
+}
+constexpr size_t kGramStagedSmemMax = 200 * 1024 + 1024;
+
+// The staged Gram (gram_staged_kernel): the distinct fields of X and Y, and a
+// chunk size and ring depth that keep about 200 KB of copies per SM in flight.
+static int gram_staged(spm_ctx *c, GramP &p, int ma, int mb) {
+  int nf = 0;
+  auto slot = [&](const void *f) {
+    for (int i = 0; i < nf; i++)
+      if (p.F[i] == f) return i;
+    p.F[nf] = f;
+    return nf++;
+  };
+  for (int a = 0; a < ma; a++) p.xf[a] = (unsigned char)slot(p.X[a]);
+  for (int b = 0; b < mb; b++) p.yf[b] = (unsigned char)slot(p.Y[b]);
+  p.nf = nf;
+  // bytes per field and chunk x buffers: 8 KB x 3 (<= 8 fields), 4 KB x 3
+  // (<= 16), 2 KB x 4 (<= 24), 2 KB x 3 (<= 32), 1 KB x 4 (<= 48); every
+  // field (N^3 points, N a multiple of 32) is a whole number of chunks
+  if (nf <= 8) p.chunk_bytes = 8192, p.stages = 3;
+  else if (nf <= 16) p.chunk_bytes = 4096, p.stages = 3;
+  else if (nf <= 24) p.chunk_bytes = 2048, p.stages = 4;
+  else if (nf <= 32) p.chunk_bytes = 2048, p.stages = 3;
+  else p.chunk_bytes = 1024, p.stages = 4;
+  const size_t esz = c->prec == SPM_FP64 ? sizeof(double) : sizeof(float);
+  if ((p.n * esz) % (size_t)p.chunk_bytes != 0)
+    return spm_fail(SPM_ERR_ARG, "field size is not a whole number of Gram chunks");
+  p.err = c->flow + FW_ERR;
+  const size_t smem = gram_staged_smem(p);
+  const int TA = (ma + 7) / 8, TB = (mb + 7) / 8;
+  cudaError_t e = cudaSuccess;
+  auto launch = [&](auto kern) {
+    // (a host-side attribute write, made at every call: all kernels of this
+    // family have one function type, so a cache per lambda type would be shared)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramStagedSmemMax);
+    if (e == cudaSuccess) kern<<<kStageBlocks, (kStageWarps + 1) * 32, smem, c->stream>>>(p);
+  };
+  auto pick = [&](auto kd, auto kf) {
+    if (c->prec == SPM_FP64) launch(kd);
+    else launch(kf);
+  };
+#define SPM_GRAM_STAGED(A, B) \
+  if (TA == A && TB == B) pick(gram_staged_kernel<double, A, B>, gram_staged_kernel<float, A, B>);
+  SPM_GRAM_STAGED(1, 1) else SPM_GRAM_STAGED(1, 2) else SPM_GRAM_STAGED(1, 3)
+  else SPM_GRAM_STAGED(2, 1) else SPM_GRAM_STAGED(2, 2) else SPM_GRAM_STAGED(2, 3)
+  else SPM_GRAM_STAGED(3, 1) else SPM_GRAM_STAGED(3, 2)
+  else return spm_fail(SPM_ERR_ARG, "staged gram: 3 x 3 tiles go to gram_kernel");
+#undef SPM_GRAM_STAGED
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "staged gram launch");
+}
+
 // G = X^T Y / N^3 (ma x mb, row-major) into host memory (synchronises).
 int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector<double> &G) {
+  if (ma < 1 || mb < 1 || ma > kBlkMax || mb > kBlkMax) return spm_fail(SPM_ERR_ARG, "gram size");
   Solver *s = solver(c);
   GramP p;
   std::memset(&p, 0, sizeof(p));
@@ -77,6 +136,21 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
   p.ticket = s->gram_ticket;
   p.out = s->gram_out;
   c->launches++;
+  // Staged through shared memory, except the 24 x 24 Rayleigh-Ritz Gram
+  // (3 x 3 tiles, 3 flop per byte): bound by the DMMA rate, it runs faster on
+  // gram_kernel's 16 warps per SM (3.5 against 3.2 TB/s at 256^3)
+  if (c->block_stage && (ma + 7) / 8 * ((mb + 7) / 8) < 9) {
+    SPM_TRY(gram_staged(c, p, ma, mb));
+    cudaError_t e = cudaMemcpyAsync(s->h_gram, s->gram_out, sizeof(double) * (ma * mb + 1), cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "gram");
+    if (s->h_gram[ma * mb] != 0.0) return spm_check_device_error(c);
+    G.assign(s->h_gram, s->h_gram + ma * mb);
+    for (double v : G)
+      if (!std::isfinite(v)) return spm_fail(SPM_ERR_NONFINITE, "non-finite Gram entry");
+    return SPM_OK;
+  }
   // blocks of up to 8 / 16 vectors: four k-steps per loop iteration; up to 24: two
   const int tiles = (std::max(ma, mb) + 7) / 8;
   // Y = X[8 yt .. 8 yt + mb) (whole tiles): Y's fields are not read again
@@ -131,6 +205,45 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
   p.accumulate = acc ? 1 : 0;
   cudaError_t e = cudaSuccess;
   c->launches++;
+  if (c->block_stage && !acc && nout <= 8 && nin > 8) {
+    // staged through shared memory (combine_staged_kernel): the distinct
+    // inputs, the coefficients repacked with row stride kBlkMax. (Eight or
+    // fewer inputs, as the in-place 8 -> 8 update of the new block, stream
+    // about as fast through combine_kernel: 5.9 against 5.5 TB/s at 256^3.)
+    int nf = 0;
+    for (int i = 0; i < nin; i++) {
+      int f = 0;
+      while (f < nf && p.F[f] != X[i]) f++;
+      if (f == nf) p.F[nf++] = X[i];
+      p.xf[i] = (unsigned char)f;
+    }
+    p.nf = nf;
+    std::fill(p.C, p.C + (kBlkMax + 8) * kBlkMax, 0.0);
+    for (int i = 0; i < nin; i++)
+      for (int q = 0; q < nout; q++) p.C[i * kBlkMax + q] = C[(size_t)i * nout + q];
+    // about 200 KB of buffers; a chunk has at least a point per thread of a group
+    if (nf <= 8) p.chunk_bytes = 4096, p.stages = 6;
+    else if (nf <= 16) p.chunk_bytes = 2048, p.stages = 6;
+    else if (nf <= 24) p.chunk_bytes = 2048, p.stages = 4;
+    else p.chunk_bytes = 2048, p.stages = 3;
+    const size_t esz = c->prec == SPM_FP64 ? sizeof(double) : sizeof(float);
+    if ((p.n * esz) % (size_t)p.chunk_bytes != 0)
+      return spm_fail(SPM_ERR_ARG, "field size is not a whole number of combination chunks");
+    p.err = c->flow + FW_ERR;
+    const size_t smem = (size_t)p.stages * nf * (p.chunk_bytes + 16) + 16 * (size_t)p.stages + 128;
+    auto launch_s = [&](auto kern) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramStagedSmemMax);
+      if (e == cudaSuccess) kern<<<kStageBlocks, (kCombWarps + 1) * 32, smem, c->stream>>>(p);
+    };
+    auto pick = [&](auto kd, auto kf) {
+      if (c->prec == SPM_FP64) launch_s(kd);
+      else launch_s(kf);
+    };
+    if (nin <= 16) pick(combine_staged_kernel<double, 16, 8>, combine_staged_kernel<float, 16, 8>);
+    else pick(combine_staged_kernel<double, kBlkMax + 8, 8>, combine_staged_kernel<float, kBlkMax + 8, 8>);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "staged combine launch");
+  }
   // register-bounded variants by block shape (two points per thread where they fit)
   auto launch = [&](auto kd, auto kf) {
     if (c->prec == SPM_FP64) kd<<<1184, 256, 0, c->stream>>>(p);
@@ -381,6 +494,34 @@ void spm_free_extra(spm_ctx *c) {
   if (s->h_gram) cudaFreeHost(s->h_gram);
   delete s;
   c->extra = nullptr;
+}
+
+extern "C" int spm_block_gram(spm_ctx *c, const void *const *X, int ma, const void *const *Y, int mb, double *G) {
+  if (!c || !X || !Y || !G || ma < 1 || mb < 1 || ma > kBlkMax || mb > kBlkMax)
+    return spm_fail(SPM_ERR_ARG, "bad argument (1 <= ma, mb <= 24)");
+  for (int i = 0; i < ma; i++)
+    if (!X[i]) return spm_fail(SPM_ERR_ARG, "null field in X");
+  for (int i = 0; i < mb; i++)
+    if (!Y[i]) return spm_fail(SPM_ERR_ARG, "null field in Y");
+  SPM_TRY(ensure_base(c));
+  std::vector<double> out;
+  SPM_TRY(gram(c, const_cast<void *const *>(X), ma, const_cast<void *const *>(Y), mb, out));
+  std::copy(out.begin(), out.end(), G);
+  return SPM_OK;
+}
+
+extern "C" int spm_block_combine(spm_ctx *c, const void *const *X, int nin, void *const *Y, int nout, const double *C,
+                                 const double *d) {
+  if (!c || !X || !Y || !C || nin < 1 || nout < 1 || nin > kBlkMax + 8 || nout > kBlkMax)
+    return spm_fail(SPM_ERR_ARG, "bad argument (1 <= nin <= 32, 1 <= nout <= 24)");
+  for (int i = 0; i < nin; i++)
+    if (!X[i]) return spm_fail(SPM_ERR_ARG, "null field in X");
+  for (int i = 0; i < nout; i++)
+    if (!Y[i]) return spm_fail(SPM_ERR_ARG, "null field in Y");
+  const std::vector<double> Cv(C, C + (size_t)nin * nout);
+  std::vector<double> dv;
+  if (d) dv.assign(d, d + nout);
+  return combine(c, const_cast<void *const *>(X), nin, Y, nout, Cv, d ? &dv : nullptr, false);
 }
 
 // ------------------------------------------------------------------ LOBPCG

@@ -389,6 +389,11 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->pencil_tc = value;
     return SPM_OK;
   }
+  if (std::strcmp(knob, "block_stage") == 0) {
+    if (value != 0 && value != 1) return spm_fail(SPM_ERR_ARG, "block_stage must be 0 or 1");
+    c->block_stage = value;
+    return SPM_OK;
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
@@ -399,6 +404,7 @@ extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (std::strcmp(knob, "plane_xg") == 0) return c->plane_xg;
   if (std::strcmp(knob, "batch_group") == 0) return c->batch_group;
   if (std::strcmp(knob, "pencil_tc") == 0) return c->pencil_tc;
+  if (std::strcmp(knob, "block_stage") == 0) return c->block_stage;
   return -1;
 }
 
@@ -590,6 +596,7 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->plane_xg = c->plane_xg;
   c->twin->batch_group = c->batch_group;
   c->twin->pencil_tc = c->pencil_tc;
+  c->twin->block_stage = c->block_stage;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
   spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg,
                       &c->twin->pencil_tc);

@@ -87,6 +87,10 @@ def lib():
             "spm_hv": [_vp, _vp, _vp, _vp, ctypes.c_int],
             "spm_precond": [_vp, _vp, ctypes.c_int],
             "spm_inpfp": [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)],
+            "spm_block_gram": [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_double)],
+            "spm_block_combine": [_vp, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
             "spm_supported_size": [ctypes.c_int],
             "spm_lobpcg_init": [_vp, _vp, ctypes.c_int, ctypes.c_uint64],
             "spm_lobpcg": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -358,6 +362,32 @@ class SpmContext:
 
     def nrmp(self, p) -> float:
         return float(np.sqrt(self.inpfp(p, p)))
+
+    def block_gram(self, X, Y) -> np.ndarray:
+        """G[a, b] = inpfp(X[a], Y[b]) for sequences of fields X, Y (at most 24 each;
+        fields may repeat and be shared between X and Y), the LOBPCG Gram."""
+        X, Y = list(X), list(Y)
+        xa = (_vp * len(X))(*[_ptr(f) for f in X])
+        ya = (_vp * len(Y))(*[_ptr(f) for f in Y])
+        G = np.zeros((len(X), len(Y)), dtype=np.float64)
+        check(lib().spm_block_gram(self.h, xa, len(X), ya, len(Y),
+                                   G.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return G
+
+    def block_combine(self, X, Y, C, d=None):
+        """Y[q] = sum_p C[p, q] X[p] + d[q] in place on the fields Y (which may be
+        fields of X), the LOBPCG block update; C is len(X) x len(Y)."""
+        X, Y = list(X), list(Y)
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        assert C.shape == (len(X), len(Y))
+        xa = (_vp * len(X))(*[_ptr(f) for f in X])
+        ya = (_vp * len(Y))(*[_ptr(f) for f in Y])
+        dp = None
+        if d is not None:
+            d = np.ascontiguousarray(d, dtype=np.float64)
+            dp = d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        check(lib().spm_block_combine(self.h, xa, len(X), ya, len(Y),
+                                      C.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), dp))
 
 
 _KINDS = {"relax": SPM_JOB_RELAX, "lobpcg": SPM_JOB_LOBPCG, "spm": SPM_JOB_SPM}

@@ -113,6 +113,98 @@ def test_inpfp(spm, cuda):
     assert abs(ctx.inpfp(t(cuda, a), t(cuda, b)) - m.inpfp(a, b)) <= 1e-12 * abs(m.inpfp(a, b))
 
 
+# block shapes of the LOBPCG Grams (as index lists into one pool of fields):
+# V^T U, V^T V, [V W]^T W, [V W P]^T P, S^T HS, ragged tiles, repeats, a shifted alias
+GRAM_SHAPES = {
+    "8x8": (list(range(8)), list(range(8, 16))),
+    "self8": (list(range(8)), list(range(8))),
+    "qx16": (list(range(16)), list(range(8, 16))),
+    "qx24": (list(range(24)), list(range(16, 24))),
+    "rr24": (list(range(24)), list(range(24, 48))),
+    "ragged": (list(range(5)), list(range(30, 43))),
+    "repeat": ([0, 0, 1, 2, 1], [2, 0]),
+    "shift": (list(range(17)), [2, 3, 4]),
+}
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("N", [32, 96])
+@pytest.mark.parametrize("shape", sorted(GRAM_SHAPES))
+def test_block_gram(spm, cuda, N, prec, shape):
+    """spm_block_gram against NumPy (the Gram of LOBPCG.cpp:336-358), with the
+    fields staged through shared memory (default) and read directly: within
+    1e-13 of sqrt(G_aa G_bb) (the FP32 fields' products are exact in the FP64
+    sums), and the same bits on a second call."""
+    xs, ys = GRAM_SHAPES[shape]
+    nfld = max(xs + ys) + 1
+    rng = np.random.default_rng(7 * N + nfld)
+    pool = rng.uniform(-1.0, 1.0, (nfld,) + (N,) * 3) + 0.3 * rng.standard_normal((nfld, 1, 1, 1))
+    if prec == "fp32":
+        pool = pool.astype(np.float32)
+    pd = t(cuda, pool)
+    flat = pool.reshape(nfld, -1).astype(np.float64)
+    ref = flat[xs] @ flat[ys].T / N ** 3
+    nrm = np.sqrt(np.einsum("ij,ij->i", flat, flat) / N ** 3)
+    scale = np.outer(nrm[xs], nrm[ys])
+    ctx = spm.SpmContext(N, precision=prec)
+    for stage in (1, 0):
+        ctx.tune("block_stage", stage)
+        G = ctx.block_gram([pd[i] for i in xs], [pd[j] for j in ys])
+        assert G.shape == ref.shape
+        assert np.max(np.abs(G - ref) / scale) < 1e-13, (stage, np.max(np.abs(G - ref) / scale))
+        G2 = ctx.block_gram([pd[i] for i in xs], [pd[j] for j in ys])
+        assert np.array_equal(G, G2)
+
+
+# (inputs, outputs) as index lists into one pool of fields; outputs that are
+# also inputs are updated in place
+COMB_SHAPES = {
+    "w16": (list(range(16)), list(range(16, 24))),
+    "p24_inplace": (list(range(24)), list(range(16, 24))),
+    "v8_inplace_d": (list(range(8)), list(range(8))),
+    "max32": (list(range(32)), list(range(32, 40))),
+    "ragged": (list(range(5)), [7, 8, 9]),
+    "wide12": (list(range(10)), list(range(10, 22))),
+    "repeat": ([0, 1, 0, 2], [3]),
+    "repeat9": ([0, 1, 2, 0, 1, 2, 3, 3, 4], [5, 6]),
+}
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("N", [32, 96])
+@pytest.mark.parametrize("shape", sorted(COMB_SHAPES))
+def test_block_combine(spm, cuda, N, prec, shape):
+    """spm_block_combine (the Ritz update of LOBPCG.cpp:403-418) against NumPy
+    within 1e-13 of sum_p |C_pq| |X_p| (FP32: the FP32 rounding of the FP64
+    result), in place where outputs are inputs; the inputs staged through
+    shared memory (default) give the same bits as the direct kernel."""
+    xs, ys = COMB_SHAPES[shape]
+    nfld = max(xs + ys) + 1
+    rng = np.random.default_rng(11 * N + nfld)
+    pool = rng.uniform(-1.0, 1.0, (nfld,) + (N,) * 3)
+    if prec == "fp32":
+        pool = pool.astype(np.float32)
+    C = rng.standard_normal((len(xs), len(ys)))
+    d = rng.standard_normal(len(ys)) if shape.endswith("_d") else None
+    flat = pool.reshape(nfld, -1).astype(np.float64)
+    ref = C.T @ flat[xs] + (0.0 if d is None else d[:, None])
+    scale = np.abs(C).T @ np.abs(flat[xs]) + 1e-300
+    tol = 1e-13 if prec == "fp64" else 2 ** -23
+    ctx = spm.SpmContext(N, precision=prec)
+    outs = []
+    for stage in (1, 0):
+        ctx.tune("block_stage", stage)
+        pd = t(cuda, pool)
+        ctx.block_combine([pd[i] for i in xs], [pd[j] for j in ys], C, d)
+        got = pd.cpu().numpy().reshape(nfld, -1)[ys].astype(np.float64)
+        assert np.max(np.abs(got - ref) / np.maximum(scale, np.abs(ref))) < tol, stage
+        # fields that are not outputs are untouched
+        others = [i for i in range(nfld) if i not in ys]
+        assert np.array_equal(pd.cpu().numpy()[others], pool[others])
+        outs.append(got)
+    assert np.array_equal(outs[0], outs[1])
+
+
 @pytest.mark.parametrize("N", [32, 64, 128, 160, 192])
 def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
     """Chains of steps with the fused inverse -> forward plane pass give the
