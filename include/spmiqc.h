@@ -234,6 +234,15 @@ int spm_lobpcg_init(spm_ctx *ctx, void *V, int k, uint64_t seed);
  * of k, may be NULL), *iters the iterations done. */
 int spm_lobpcg(spm_ctx *ctx, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
                double *resid, int *iters);
+/* spm_lobpcg with guard vectors, for solves run to a tolerance: V holds
+ * k + guard fields (k + guard <= 8, start block from spm_lobpcg_init of
+ * k + guard) and the iteration runs on the whole block, but the stop test
+ * takes only the first k residuals. Where the k-th eigenvalue has a close
+ * neighbour above it, a block of k converges slowly (its last vector mixes
+ * with the neighbour); the guards hold the neighbours. evals and resid (may
+ * be NULL) receive k + guard entries. guard = 0 is spm_lobpcg. */
+int spm_lobpcg_guarded(spm_ctx *ctx, const void *phi, void *V, int k, int guard, int maxiter, double tol,
+                       double *evals, double *resid, int *iters);
 
 /* ------------------------------------------------------------------ SPM */
 
@@ -367,7 +376,7 @@ typedef struct spm_job_desc {
   int precision;   /* SPM_FP64, SPM_FP32 or SPM_MIXED (relaxation and SPM) */
   int k;           /* LOBPCG block size, 1..8 */
   int max_steps;   /* step / iteration cap */
-  int reserved;
+  int guard;       /* LOBPCG guard vectors (spm_lobpcg_guarded), k + guard <= 8; 0 for other jobs */
   double L, Tau, Gamma, dt;
   double tol;        /* ||grad F|| (relaxation), residual (LOBPCG, SPM) */
   double switch_tol; /* SPM_MIXED: FP32 until this tolerance (0: as far as FP32 goes) */

@@ -63,9 +63,11 @@ size_t footprint_of(const spm_job_desc &d) {
     case SPM_JOB_RELAX:  // phi, uhat, gradient; scratch 2; FP32 twin: 2 half fields + scratch
       fields = 3 + 2 + (mixed ? 1 + 1 : 0);
       break;
-    case SPM_JOB_LOBPCG:  // phi, V (k), work 6k, scratch 2 per batched vector
-      fields = 1 + d.k + 6.0 * d.k + 2.0 * d.k + 1;
+    case SPM_JOB_LOBPCG: {  // phi, V (k + guard), work 6 per vector, scratch 2 per batched vector
+      const double kb = d.k + d.guard;
+      fields = 1 + kb + 6.0 * kb + 2.0 * kb + 1;
       break;
+    }
     case SPM_JOB_SPM:  // replicas 2, uhat, v/vhat/Gv, scratch 2 x 2; twin half of that
       fields = 2 + 1 + 3 + 4 + (mixed ? 1 + 3.5 : 0);
       break;
@@ -126,7 +128,7 @@ int run_job_gpu(spm_server *S, Job *j) {
   spm_ctx *c = R.c;
   c->cancel = &j->cancel;
   const size_t fb = n * rb;
-  const int nf = d.kind == SPM_JOB_LOBPCG ? 1 + d.k : 3;
+  const int nf = d.kind == SPM_JOB_LOBPCG ? 1 + d.k + d.guard : 3;  // phi and V (with its guard vectors)
   e = cudaMalloc(&R.buf, fb * (size_t)nf);
   if (e != cudaSuccess) return spm_fail(SPM_ERR_NOMEM, "job fields");
   char *b = (char *)R.buf;
@@ -177,9 +179,9 @@ int run_job_gpu(spm_server *S, Job *j) {
     JOB_TRY(download(phi, n));
   } else if (d.kind == SPM_JOB_LOBPCG) {
     void *phi = b, *V = b + fb;
-    JOB_TRY(spm_lobpcg_init(c, V, d.k, d.seed));
+    JOB_TRY(spm_lobpcg_init(c, V, d.k + d.guard, d.seed));
     double rs[8] = {0};
-    JOB_TRY(spm_lobpcg(c, phi, V, d.k, d.max_steps, d.tol, j->r.evals, rs, &j->r.steps));
+    JOB_TRY(spm_lobpcg_guarded(c, phi, V, d.k, d.guard, d.max_steps, d.tol, j->r.evals, rs, &j->r.steps));
     for (int i = 0; i < d.k; i++) j->r.residual = std::max(j->r.residual, rs[i]);
     JOB_TRY(download(V, n * (size_t)d.k));
   } else {
@@ -211,7 +213,7 @@ int run_job_fake(spm_server *S, Job *j) {
       return SPM_ERR_NOMEM;  // the device refused the allocation
     S->fake_used += j->footprint;
   }
-  const double units = (double)npts(d.N) / 1e6 * std::max(d.max_steps, 0) * (d.kind == SPM_JOB_LOBPCG ? d.k : 1);
+  const double units = (double)npts(d.N) / 1e6 * std::max(d.max_steps, 0) * (d.kind == SPM_JOB_LOBPCG ? d.k + d.guard : 1);
   const auto end = Clock::now() + std::chrono::duration<double, std::milli>(S->cfg.fake_ms_per_munit * units);
   int rc = SPM_OK;
   while (Clock::now() < end) {
@@ -337,7 +339,9 @@ extern "C" int spm_server_submit(spm_server *S, const spm_job_desc *d, const dou
   if (!spm_supported_size(d->N)) return spm_fail(SPM_ERR_UNSUPPORTED, "grid size not built");
   if (d->kind < SPM_JOB_RELAX || d->kind > SPM_JOB_SPM) return spm_fail(SPM_ERR_ARG, "unknown job kind");
   if (d->precision < SPM_FP64 || d->precision > SPM_MIXED) return spm_fail(SPM_ERR_ARG, "unknown precision");
-  if (d->kind == SPM_JOB_LOBPCG && (d->k < 1 || d->k > 8)) return spm_fail(SPM_ERR_ARG, "k must be in [1, 8]");
+  if (d->kind == SPM_JOB_LOBPCG && (d->k < 1 || d->guard < 0 || d->k + d->guard > 8))
+    return spm_fail(SPM_ERR_ARG, "LOBPCG jobs need k >= 1, guard >= 0 and k + guard <= 8");
+  if (d->kind != SPM_JOB_LOBPCG && d->guard != 0) return spm_fail(SPM_ERR_ARG, "guard is for LOBPCG jobs");
   if (d->kind == SPM_JOB_LOBPCG && d->precision == SPM_MIXED)
     return spm_fail(SPM_ERR_ARG, "LOBPCG jobs run in FP64 or FP32");
   if (d->kind == SPM_JOB_SPM && !phi1) return spm_fail(SPM_ERR_ARG, "a saddle search needs two replicas");

@@ -733,33 +733,48 @@ static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &ha
   return orthonormalize(c, B.Vc.data(), k);
 }
 
-extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
-                          double *resid, int *iters) {
-  if (!c || !phi || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0)
-    return spm_fail(SPM_ERR_ARG, "bad argument (k must be in [1, 8])");
+// The LOBPCG iteration on a block of kb vectors, stopping when the first
+// nconv residuals are <= tol (nconv = kb: the reference's block; nconv < kb:
+// the others are guard vectors).
+static int lobpcg_run(spm_ctx *c, const void *phi, void *V, int kb, int nconv, int maxiter, double tol,
+                      double *evals, double *resid, int *iters) {
   SPM_TRY(ensure_base(c));
   LobBlocks B;
-  SPM_TRY(lob_blocks(c, V, k, B));
-  std::vector<double> alpha(k, 0.0), res(k, 0.0);
-  SPM_TRY(orthonormalize(c, B.Vc.data(), k));  // LOBPCG.cpp:262-267
+  SPM_TRY(lob_blocks(c, V, kb, B));
+  std::vector<double> alpha(kb, 0.0), res(kb, 0.0);
+  SPM_TRY(orthonormalize(c, B.Vc.data(), kb));  // LOBPCG.cpp:262-267
   int it = 0;
   bool have_p = false;
   for (;; it++) {
-    SPM_TRY(lob_residual(c, phi, B, k, alpha, res));
+    SPM_TRY(lob_residual(c, phi, B, kb, alpha, res));
     double rmax = 0.0;
-    for (int i = 0; i < k; i++) rmax = std::max(rmax, res[i]);
+    for (int i = 0; i < nconv; i++) rmax = std::max(rmax, res[i]);
     if (it >= maxiter || (tol > 0 && rmax <= tol)) break;
     if (spm_cancelled(c)) return spm_fail(SPM_ERR_CANCELLED, "cancelled");
-    SPM_TRY(lob_update(c, phi, B, k, have_p));
+    SPM_TRY(lob_update(c, phi, B, kb, have_p));
   }
   // the caller's buffer receives the final block
-  for (int i = 0; i < k; i++) SPM_TRY(copy_fields(c, fld(c, V, i), B.Vc[i], 1));
+  for (int i = 0; i < kb; i++) SPM_TRY(copy_fields(c, fld(c, V, i), B.Vc[i], 1));
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "lobpcg");
   if (evals) std::copy(alpha.begin(), alpha.end(), evals);
   if (resid) std::copy(res.begin(), res.end(), resid);
   if (iters) *iters = it;
   return SPM_OK;
+}
+
+extern "C" int spm_lobpcg(spm_ctx *c, const void *phi, void *V, int k, int maxiter, double tol, double *evals,
+                          double *resid, int *iters) {
+  if (!c || !phi || !V || k < 1 || k > kBlkMax / 3 || maxiter < 0)
+    return spm_fail(SPM_ERR_ARG, "bad argument (k must be in [1, 8])");
+  return lobpcg_run(c, phi, V, k, k, maxiter, tol, evals, resid, iters);
+}
+
+extern "C" int spm_lobpcg_guarded(spm_ctx *c, const void *phi, void *V, int k, int guard, int maxiter, double tol,
+                                  double *evals, double *resid, int *iters) {
+  if (!c || !phi || !V || k < 1 || guard < 0 || k + guard > kBlkMax / 3 || maxiter < 0)
+    return spm_fail(SPM_ERR_ARG, "bad argument (k >= 1, guard >= 0, k + guard <= 8)");
+  return lobpcg_run(c, phi, V, k + guard, k, maxiter, tol, evals, resid, iters);
 }
 
 // ------------------------------------------------------------------ SPM

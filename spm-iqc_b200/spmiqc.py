@@ -39,7 +39,7 @@ class StepStats(ctypes.Structure):
 
 class JobDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("N", ctypes.c_int), ("precision", ctypes.c_int), ("k", ctypes.c_int),
-                ("max_steps", ctypes.c_int), ("reserved", ctypes.c_int), ("L", ctypes.c_double),
+                ("max_steps", ctypes.c_int), ("guard", ctypes.c_int), ("L", ctypes.c_double),
                 ("Tau", ctypes.c_double), ("Gamma", ctypes.c_double), ("dt", ctypes.c_double),
                 ("tol", ctypes.c_double), ("switch_tol", ctypes.c_double), ("seed", ctypes.c_uint64)]
 
@@ -289,6 +289,20 @@ class SpmContext:
                                ctypes.byref(it)))
         return np.array(ev[:]), np.array(rs[:]), it.value
 
+    def lobpcg_guarded(self, phi, V, k: int, maxiter: int = 400, tol: float = 1e-8):
+        """LOBPCG on the whole block V (k + guard fields) stopping when the first
+        k residuals are <= tol; returns (evals, residuals, iterations) of the
+        whole block."""
+        kb = V.shape[0]
+        ev = (ctypes.c_double * kb)()
+        rs = (ctypes.c_double * kb)()
+        it = ctypes.c_int()
+        f = lib().spm_lobpcg_guarded
+        f.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+        check(f(self.h, _ptr(phi), _ptr(V), int(k), int(kb - k), int(maxiter), float(tol), ev, rs, ctypes.byref(it)))
+        return np.array(ev[:]), np.array(rs[:]), it.value
+
     # ---- SPM.cpp
     def hiosd_lobpcg_sieh(self, x, V, dt: float = 0.8, betat: float = 8.0, betau: float = 0.02,
                           epsf: float = 1e-7, maxiter: int = 10000):
@@ -396,9 +410,10 @@ _PRECS = {"fp64": SPM_FP64, "fp32": SPM_FP32, "mixed": SPM_MIXED}
 
 def job_desc(kind: str, N: int, precision: str = "fp64", k: int = 4, max_steps: int = 1000, L: float = 26.0,
              Tau: float = -0.0061, Gamma: float = 0.30, dt: float = 0.3, tol: float = 1e-8,
-             switch_tol: float = 0.0, seed: int = 0) -> JobDesc:
-    return JobDesc(_KINDS[kind], int(N), _PRECS[precision], int(k), int(max_steps), 0, float(L), float(Tau),
-                   float(Gamma), float(dt), float(tol), float(switch_tol), int(seed))
+             switch_tol: float = 0.0, seed: int = 0, guard: int = 0) -> JobDesc:
+    """guard: LOBPCG guard vectors (k + guard <= 8), see lobpcg_guarded."""
+    return JobDesc(_KINDS[kind], int(N), _PRECS[precision], int(k), int(max_steps), int(guard), float(L),
+                   float(Tau), float(Gamma), float(dt), float(tol), float(switch_tol), int(seed))
 
 
 def job_footprint(desc: JobDesc) -> int:

@@ -162,3 +162,36 @@ def test_gosd_matches_oracle(spm, cuda):
     Vg = V.cpu().numpy()
     assert min(rel(Vg[0], Vo[0]), rel(-Vg[0], Vo[0])) < 1e-8
     assert max(abs(m.inpfp(Vg[0], V00[i])) for i in range(2)) < 1e-12
+
+
+def test_lobpcg_guard_vectors_converge_a_close_pair(spm, cuda):
+    """A k = 4 solve whose 4th eigenvalue has a close neighbour (a cosine-shell
+    field of the serving stream, N = 64): the block of 4 stalls far above 1e-8
+    within 400 iterations, the block of 8 with the stop test on the first 4
+    (spm_lobpcg_guarded) reaches it. The returned pairs are checked directly,
+    ||H v_i - lambda_i v_i|| through the Hessian product, and the converged
+    eigenvalues agree between the two runs; guard = 0 is spm_lobpcg."""
+    import workloads
+    spec = next(s for s in workloads.serving_stream(seed=2024, n_jobs=32) if s.kind == "lobpcg" and s.N == 64)
+    ctx = spm.SpmContext(64, L=spec.L, Tau=spec.Tau)
+    phi = t(cuda, workloads.field(spec))
+    V4 = ctx.hiosd_lobpcg_initialization(4, seed=spec.seed)
+    ev4, rs4, it4 = ctx.hiosd_lobpcg_inip(phi, V4, maxiter=400, tol=1e-8)
+    assert it4 == 400 and rs4[3] > 1e-6
+    V8 = ctx.hiosd_lobpcg_initialization(8, seed=spec.seed)
+    ev8, rs8, it8 = ctx.lobpcg_guarded(phi, V8, 4, maxiter=400, tol=1e-8)
+    assert it8 < 400 and max(rs8[:4]) <= 1e-8
+    HV = ctx.hv_cam(phi, V8[:4].contiguous())
+    for i in range(4):
+        r = HV[i] - float(ev8[i]) * V8[i]
+        assert ctx.nrmp(r) <= 2e-8 * max(1.0, abs(ev8[i]))
+        assert abs(ctx.nrmp(V8[i]) - 1.0) < 1e-12
+    # the pairs the block of 4 did converge are the same eigenvalues
+    assert np.max(np.abs(ev8[:3] - ev4[:3]) / np.abs(ev4[:3])) < 1e-10
+    # no guards: the same iteration as spm_lobpcg
+    Va = ctx.hiosd_lobpcg_initialization(3, seed=1)
+    Vb = Va.clone()
+    a = ctx.hiosd_lobpcg_inip(phi, Va, maxiter=5)
+    b = ctx.lobpcg_guarded(phi, Vb, 3, maxiter=5, tol=0.0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    assert cuda.equal(Va, Vb)

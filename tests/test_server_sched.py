@@ -141,6 +141,24 @@ def test_job_larger_than_budget_is_refused_at_submission():
             srv.submit(job_desc("spm", 64), _phi(64))      # needs two replicas
 
 
+def test_lobpcg_guard_vectors_are_checked_and_counted():
+    """A LOBPCG job's guard vectors add to its footprint; k + guard above 8,
+    a negative guard, or a guard on another kind of job is refused; the job
+    returns its k vectors."""
+    fp4 = job_footprint(job_desc("lobpcg", 128, k=4))
+    fp8 = job_footprint(job_desc("lobpcg", 128, k=8))
+    assert job_footprint(job_desc("lobpcg", 128, k=4, guard=4)) == fp8 > fp4
+    with JobServer(budget_bytes=1 << 40, max_slots=2, fake_device=True, fake_ms_per_munit=0.01) as srv:
+        for bad in (job_desc("lobpcg", 64, k=6, guard=3), job_desc("lobpcg", 64, k=4, guard=-1),
+                    job_desc("relax", 64, guard=2)):
+            with pytest.raises(spmiqc.SpmError) as e:
+                srv.submit(bad, _phi(64))
+            assert e.value.status == spmiqc.SPM_ERR_ARG
+        j = srv.submit(job_desc("lobpcg", 32, k=3, guard=2, max_steps=5), _phi(32, 0.5))
+        r, V = srv.wait(j)
+    assert r.status == 0 and V.shape == (3, 32, 32, 32)
+
+
 def test_latency_percentiles_and_results():
     rng = np.random.default_rng(3)
     with JobServer(budget_bytes=1 << 40, max_slots=2, fake_device=True, fake_ms_per_munit=1.0) as srv:
