@@ -258,6 +258,15 @@ int spm_minmax_forces(spm_ctx *ctx, void *x, const void *v);
  * iteration; *iters the iterations done. */
 int spm_spring_pairing(spm_ctx *ctx, void *phi0, void *phi1, int maxiter, double tol, double *res_hist,
                        int *iters);
+/* Rest length of the spring between the SPM replicas (default 0: the
+ * reference's spring, whose rest length spring_d = 0.001 is computed into
+ * kd = ks (dd - spring_d) but never applied, SPM.cpp:179, 206-212). With
+ * rest > 0 both spring updates of an iteration apply the force
+ * ks (dd - rest) along (phi1 - phi0) / dd, dd = nrmp(phi1 - phi0) measured
+ * after the natural-force step, so the pair settles at distance ~rest
+ * around the saddle instead of collapsing onto it. Applies to
+ * spm_spring_pairing and spm_spring_pairing_mixed on this context. */
+int spm_set_spring_length(spm_ctx *ctx, double rest);
 /* Mixed-precision Spring_Pairing (no counterpart in the reference): on an
  * FP64 context, the natural-force and min-max steps run with FP32 transforms
  * (FP64 reductions) until res <= max(switch_tol, tol) or until 256 FP32

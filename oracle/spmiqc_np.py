@@ -361,8 +361,11 @@ class Model:
         return self.force_step(x, v, 2.0)
 
     # src/SPM.cpp:170-263
-    def spring_pairing(self, phi0, phi1, maxiter, tol):
-        """Returns (phi0, phi1, iterations, last residual)."""
+    def spring_pairing(self, phi0, phi1, maxiter, tol, rest: float = 0.0):
+        """Returns (phi0, phi1, iterations, last residual). rest > 0: a spring of
+        that rest length, the reference's unused kd = ks (dd - spring_d)
+        (SPM.cpp:199-212) applied along (phi1 - phi0) / dd, with dd measured
+        once per iteration after the natural-force step."""
         dt, ks = 0.001, 1.0
         P = [phi0.copy(), phi1.copy()]
         res, it = 1e-6, 0
@@ -371,6 +374,9 @@ class Model:
             v = self.tangent(P[0], P[1])
             for i in range(2):
                 P[i] = self.natural_forces(P[i], v)
+            if rest > 0:
+                dd = self.nrmp(P[1] - P[0])
+                ks = 1.0 * ((dd - rest) / dd) if dd > 0 else 0.0
             for i in range(2):
                 Fs = ks * P[1] + (-ks) * P[0] if i == 0 else ks * P[0] + (-ks) * P[1]
                 P[i] = 1 * P[i] + dt * Fs

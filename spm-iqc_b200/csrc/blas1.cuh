@@ -42,6 +42,22 @@ template <class T> struct ProDot {
   }
 };
 
+// Squared distance of an SPM replica pair, ||phi1 - phi0||^2 under inpfp
+// (the dd of SPM.cpp:199-200): in = phi0, aux0 = phi1.
+template <class T> struct ProDist {
+  static constexpr int NR = 1;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> pro(const KParams &p, int b, size_t idx, c2<T> x, double (&acc)[1]) {
+    const c2<T> q = __ldg(reinterpret_cast<const c2<T> *>(reinterpret_cast<const T *>(p.aux0[b]) + idx));
+    const double dx = (double)q.x - (double)x.x, dy = (double)q.y - (double)x.y;
+    acc[0] += dx * dx + dy * dy;
+    return x;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
+    p.scal[(size_t)b * kScal + SC_DD] = tot[0] * p.m.inv_n3;
+  }
+};
+
 // Field mean (mean_Cplx, BasicOperators.cpp:121-130): scal[SC_SUM0] = sum / N^3.
 template <class T> struct ProSum {
   static constexpr int NR = 1;

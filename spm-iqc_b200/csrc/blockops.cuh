@@ -505,11 +505,21 @@ __global__ void lobpcg_random_kernel(T *V, int k, size_t n, unsigned long long s
 }
 
 // The two spring updates of Spring_Pairing (SPM.cpp:203-216), in the
-// reference's sequential order: phi1 sees the updated phi0.
+// reference's sequential order: phi1 sees the updated phi0. dd2 (optional):
+// the pair's squared distance, for a spring of rest length `rest` (the
+// reference's spring_d and kd = ks (dd - spring_d), SPM.cpp:179, 206-212,
+// which it computes but does not apply): the force ks (dd - rest) along the
+// unit vector (phi1 - phi0) / dd, i.e. the coefficient ks (dd - rest) / dd.
 template <class T>
-__global__ void spring_kernel(T *phi0, T *phi1, size_t n, double dt, double ks, const int *flow) {
+__global__ void spring_kernel(T *phi0, T *phi1, size_t n, double dt, double ks, const int *flow,
+                              const double *dd2 = nullptr, double rest = 0.0) {
   if (flow && *((volatile const int *)flow) == 0) return;
-  const T k = (T)ks, t = (T)dt;
+  double kc = ks;
+  if (dd2) {
+    const double dd = sqrt(*dd2);
+    kc = dd > 0.0 ? ks * ((dd - rest) / dd) : 0.0;
+  }
+  const T k = (T)kc, t = (T)dt;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     T p0 = phi0[i], p1 = phi1[i];
     T fs = k * p1 + (-k) * p0;

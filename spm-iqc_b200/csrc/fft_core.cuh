@@ -47,6 +47,7 @@ enum Slot {
   SC_MU = 4,    // mean removed by an epilogue (the P0 projector)
   SC_S = 5,     // <f, v> projection coefficient of the SPM force steps
   SC_NRM2 = 6,  // squared norm (tangent)
+  SC_DD = 7,    // ||phi1 - phi0||^2 of an SPM replica pair (spring with a rest length)
   SC_SUM0 = 8,  // raw sums for host-side use
   SC_SUM1 = 9,
   SC_SUM2 = 10,

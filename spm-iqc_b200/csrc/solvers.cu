@@ -832,22 +832,45 @@ static int spm_iteration(spm_ctx *c, void *phi0, void *phi1, double tol, int cap
   const double dt = 0.001, ks = 1.0;  // SPM.cpp:177-178
   SPM_TRY(t->tangent(c, phi0, phi1, v, vh, gv));
   SPM_TRY(t->force(c, X, 2, v, vh, gv, 1.0));
-  c->launches++;
-  if (c->prec == SPM_FP64)
-    spring_kernel<double><<<1184, 256, 0, c->stream>>>((double *)phi0, (double *)phi1, n, dt, ks, c->gate);
-  else
-    spring_kernel<float><<<1184, 256, 0, c->stream>>>((float *)phi0, (float *)phi1, n, dt, ks, c->gate);
+  // a spring with a rest length: dd = ||phi1 - phi0|| after the natural-force
+  // step (SPM.cpp:199-200), used by both spring updates of the iteration
+  const double *dd2 = nullptr;
+  if (c->spring_len > 0) {
+    KParams p = spm_params(c);
+    p.in[0] = phi0;
+    p.aux0[0] = phi1;
+    c->launches++;
+    if (c->prec == SPM_FP64)
+      field_reduce_kernel<double, ProDist<double>><<<dim3(kReduceBlocks, 1), kThreads, 0, c->stream>>>(p, n / 2);
+    else
+      field_reduce_kernel<float, ProDist<float>><<<dim3(kReduceBlocks, 1), kThreads, 0, c->stream>>>(p, n / 2);
+    dd2 = c->scal + SC_DD;
+  }
+  auto spring = [&]() {
+    c->launches++;
+    if (c->prec == SPM_FP64)
+      spring_kernel<double><<<1184, 256, 0, c->stream>>>((double *)phi0, (double *)phi1, n, dt, ks, c->gate, dd2,
+                                                         c->spring_len);
+    else
+      spring_kernel<float><<<1184, 256, 0, c->stream>>>((float *)phi0, (float *)phi1, n, dt, ks, c->gate, dd2,
+                                                        c->spring_len);
+  };
+  spring();
   SPM_TRY(t->tangent(c, phi0, phi1, v, vh, gv));
   SPM_TRY(t->force(c, X, 2, v, vh, gv, 2.0));
   SPM_TRY(t->gnorm(c, (const void *const *)X, 2));
-  c->launches += 2;
-  if (c->prec == SPM_FP64)
-    spring_kernel<double><<<1184, 256, 0, c->stream>>>((double *)phi0, (double *)phi1, n, dt, ks, c->gate);
-  else
-    spring_kernel<float><<<1184, 256, 0, c->stream>>>((float *)phi0, (float *)phi1, n, dt, ks, c->gate);
+  c->launches++;
+  spring();
   spm_check_kernel<<<1, 1, 0, c->stream>>>(c->scal, c->gate, s->spm_stats, tol, cap);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "spm iteration");
+}
+
+extern "C" int spm_set_spring_length(spm_ctx *c, double rest) {
+  if (!c || !(rest >= 0) || !std::isfinite(rest)) return spm_fail(SPM_ERR_ARG, "rest length must be finite and >= 0");
+  c->spring_len = rest;
+  if (c->twin) c->twin->spring_len = rest;
+  return SPM_OK;
 }
 
 extern "C" int spm_spring_pairing(spm_ctx *c, void *phi0, void *phi1, int maxiter, double tol, double *res_hist,

@@ -597,6 +597,7 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->batch_group = c->batch_group;
   c->twin->pencil_tc = c->pencil_tc;
   c->twin->block_stage = c->block_stage;
+  c->twin->spring_len = c->spring_len;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
   spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg,
                       &c->twin->pencil_tc);

@@ -57,6 +57,7 @@ struct spm_ctx {
   int batch_group = 1;          // spm_batch_grad_flow: same-size instances share launches (knob "batch_group")
   int pencil_tc = 8;            // pencil tile width in complex columns: 8 or 4 (knob "pencil_tc")
   int block_stage = 1;          // solver Grams stage their fields through shared memory (knob "block_stage")
+  double spring_len = 0.0;      // SPM spring rest length (0: the reference's zero-length spring)
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
   const volatile int *cancel = nullptr;  // host flag polled between chunks of steps (job server)

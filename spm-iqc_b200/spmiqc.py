@@ -344,6 +344,12 @@ class SpmContext:
         check(lib().spm_minmax_forces(self.h, _ptr(x), _ptr(v)))
         return x
 
+    def set_spring_length(self, rest: float):
+        """Rest length of the SPM spring (0: the reference's zero-length spring)."""
+        f = lib().spm_set_spring_length
+        f.argtypes = [_vp, ctypes.c_double]
+        check(f(self.h, float(rest)))
+
     def Spring_Pairing(self, phi0, phi1, maxiter: int, tol: float):
         """Runs the spring pair iteration in place; returns the residual history."""
         hist = (ctypes.c_double * max(1, maxiter))()

@@ -110,6 +110,35 @@ def test_spring_pairing(spm, cuda, N):
     assert rel(p0.cpu().numpy(), a) < TOL and rel(p1.cpu().numpy(), b) < TOL
 
 
+@pytest.mark.parametrize("N", [32, 64])
+def test_spring_pairing_with_rest_length(spm, cuda, N):
+    """The opt-in spring rest length (spm_set_spring_length) against the
+    oracle's restatement: 4 iterations from replicas 0.05 apart with rest
+    length 0.1 (the spring pushes them apart), and 0 restores the reference's
+    spring bit for bit."""
+    m = npo.Model(N)
+    phi = npo.uniform_field(N, 9)
+    vr = m.tangent(phi, phi + npo.uniform_field(N, 10, amp=1.0))
+    out = {}
+    for rest in (0.1, 0.0):
+        ctx = spm.SpmContext(N)
+        ctx.set_spring_length(rest)
+        p0, p1 = t(cuda, phi), t(cuda, phi + 0.05 * vr)
+        hist = ctx.Spring_Pairing(p0, p1, 4, 1e-9)
+        a, b, it, res = m.spring_pairing(phi, phi + 0.05 * vr, 4, 1e-9, rest=rest)
+        assert len(hist) == it == 4
+        assert abs(hist[-1] - res) <= 1e-9 * res
+        assert rel(p0.cpu().numpy(), a) < TOL and rel(p1.cpu().numpy(), b) < TOL
+        out[rest] = (p0.cpu().numpy(), p1.cpu().numpy(), m.nrmp(b - a))
+    assert out[0.1][2] > out[0.0][2]  # the rest length keeps the pair further apart
+    ctx = spm.SpmContext(N)
+    p0, p1 = t(cuda, phi), t(cuda, phi + 0.05 * vr)
+    ctx.Spring_Pairing(p0, p1, 4, 1e-9)
+    assert np.array_equal(p0.cpu().numpy(), out[0.0][0]) and np.array_equal(p1.cpu().numpy(), out[0.0][1])
+    with pytest.raises(spm.SpmError):
+        ctx.set_spring_length(-1.0)
+
+
 def test_spring_pairing_stops_at_tolerance(spm, cuda):
     N = 32
     m = npo.Model(N)
