@@ -85,13 +85,16 @@ static int gram_staged(spm_ctx *c, GramP &p, int ma, int mb) {
   for (int b = 0; b < mb; b++) p.yf[b] = (unsigned char)slot(p.Y[b]);
   p.nf = nf;
   // bytes per field and chunk x buffers: 8 KB x 3 (<= 8 fields), 4 KB x 3
-  // (<= 16), 2 KB x 4 (<= 24), 2 KB x 3 (<= 32), 1 KB x 4 (<= 48); every
-  // field (N^3 points, N a multiple of 32) is a whole number of chunks
+  // (<= 16), 4 KB x 2 (<= 24), 2 KB x 3 (<= 32), 2 KB x 2 (<= 48): the largest
+  // copies that leave two buffers (bulk copies of 1-2 KB held the 24- and
+  // 48-field Grams to 3.2-4.9 TB/s at 256^3, 4 and 2 KB copies run them at
+  // 6.4 and 5.8); every field (N^3 points, N a multiple of 32) is a whole
+  // number of chunks
   if (nf <= 8) p.chunk_bytes = 8192, p.stages = 3;
   else if (nf <= 16) p.chunk_bytes = 4096, p.stages = 3;
-  else if (nf <= 24) p.chunk_bytes = 2048, p.stages = 4;
+  else if (nf <= 24) p.chunk_bytes = 4096, p.stages = 2;
   else if (nf <= 32) p.chunk_bytes = 2048, p.stages = 3;
-  else p.chunk_bytes = 1024, p.stages = 4;
+  else p.chunk_bytes = 2048, p.stages = 2;
   const size_t esz = c->prec == SPM_FP64 ? sizeof(double) : sizeof(float);
   if ((p.n * esz) % (size_t)p.chunk_bytes != 0)
     return spm_fail(SPM_ERR_ARG, "field size is not a whole number of Gram chunks");
@@ -113,8 +116,7 @@ static int gram_staged(spm_ctx *c, GramP &p, int ma, int mb) {
   if (TA == A && TB == B) pick(gram_staged_kernel<double, A, B>, gram_staged_kernel<float, A, B>);
   SPM_GRAM_STAGED(1, 1) else SPM_GRAM_STAGED(1, 2) else SPM_GRAM_STAGED(1, 3)
   else SPM_GRAM_STAGED(2, 1) else SPM_GRAM_STAGED(2, 2) else SPM_GRAM_STAGED(2, 3)
-  else SPM_GRAM_STAGED(3, 1) else SPM_GRAM_STAGED(3, 2)
-  else return spm_fail(SPM_ERR_ARG, "staged gram: 3 x 3 tiles go to gram_kernel");
+  else SPM_GRAM_STAGED(3, 1) else SPM_GRAM_STAGED(3, 2) else SPM_GRAM_STAGED(3, 3)
 #undef SPM_GRAM_STAGED
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "staged gram launch");
@@ -136,10 +138,7 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
   p.ticket = s->gram_ticket;
   p.out = s->gram_out;
   c->launches++;
-  // Staged through shared memory, except the 24 x 24 Rayleigh-Ritz Gram
-  // (3 x 3 tiles, 3 flop per byte): bound by the DMMA rate, it runs faster on
-  // gram_kernel's 16 warps per SM (3.5 against 3.2 TB/s at 256^3)
-  if (c->block_stage && (ma + 7) / 8 * ((mb + 7) / 8) < 9) {
+  if (c->block_stage) {
     SPM_TRY(gram_staged(c, p, ma, mb));
     cudaError_t e = cudaMemcpyAsync(s->h_gram, s->gram_out, sizeof(double) * (ma * mb + 1), cudaMemcpyDeviceToHost,
                                     c->stream);
