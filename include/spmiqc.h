@@ -104,6 +104,9 @@ const char *spm_status_str(int status);
  * CTAs share an SM (the same bits either way).
  * knob "batch_group" (1 or 0): spm_batch_grad_flow lets instances of the same
  * N and precision share every launch (1) or gives each its own (0).
+ * knob "block_stage" (1 or 0): the LOBPCG block kernels (Grams, combinations
+ * of more than 8 fields) stage their fields through shared memory with bulk
+ * copies (1) or load them directly (0).
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);
