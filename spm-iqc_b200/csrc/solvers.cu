@@ -341,49 +341,56 @@ void gs_coefficients(const std::vector<double> &G, int k, double thr, std::vecto
 // Symmetric eigenproblem by cyclic Jacobi; eigenvalues ascending, vectors as
 // columns of V (row-major n x n). Replaces Eigen's EigenSolver on the
 // symmetrised Rayleigh-Ritz matrix (LOBPCG.cpp:357-382), whose spectrum is real.
+// A pair (p, q) is rotated only while |a_pq| exceeds 1e-17 sqrt(|a_pp a_qq|)
+// (the relative test that keeps Jacobi's relative accuracy for the small
+// eigenvalues of a graded matrix); the sweeps stop when none is rotated. The
+// Rayleigh-Ritz matrices span many orders of magnitude (the W block's large
+// Hessian components against the wanted eigenvalues near zero), where a test
+// on the whole off-diagonal norm kept every pair rotating for a dozen sweeps.
 void sym_eig(std::vector<double> A, int n, std::vector<double> &vals, std::vector<double> &V) {
   V.assign((size_t)n * n, 0.0);
   for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
-  auto a = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+  double *a = A.data(), *v = V.data();
   for (int sweep = 0; sweep < 100; sweep++) {
-    double off = 0.0, tot = 0.0;
-    for (int i = 0; i < n; i++)
-      for (int j = 0; j < n; j++) {
-        tot += a(i, j) * a(i, j);
-        if (i != j) off += a(i, j) * a(i, j);
-      }
-    if (off <= 1e-32 * tot || off == 0.0) break;
+    int rotated = 0;
     for (int p = 0; p < n - 1; p++)
       for (int q = p + 1; q < n; q++) {
-        const double apq = a(p, q);
-        if (apq == 0.0) continue;
-        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double apq = a[(size_t)p * n + q];
+        const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
+        if (!(std::fabs(apq) > 1e-17 * std::sqrt(std::fabs(app * aqq))) || apq == 0.0) continue;
+        rotated++;
+        const double theta = (aqq - app) / (2.0 * apq);
         const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
         const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
-        for (int k = 0; k < n; k++) {
-          const double akp = a(k, p), akq = a(k, q);
-          a(k, p) = cs * akp - sn * akq;
-          a(k, q) = sn * akp + cs * akq;
+        for (int k = 0; k < n; k++) {  // columns p, q
+          double *rk = a + (size_t)k * n;
+          const double akp = rk[p], akq = rk[q];
+          rk[p] = cs * akp - sn * akq;
+          rk[q] = sn * akp + cs * akq;
+        }
+        double *rp = a + (size_t)p * n, *rq = a + (size_t)q * n;
+        for (int k = 0; k < n; k++) {  // rows p, q
+          const double apk = rp[k], aqk = rq[k];
+          rp[k] = cs * apk - sn * aqk;
+          rq[k] = sn * apk + cs * aqk;
         }
         for (int k = 0; k < n; k++) {
-          const double apk = a(p, k), aqk = a(q, k);
-          a(p, k) = cs * apk - sn * aqk;
-          a(q, k) = sn * apk + cs * aqk;
-        }
-        for (int k = 0; k < n; k++) {
-          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
-          V[(size_t)k * n + p] = cs * vkp - sn * vkq;
-          V[(size_t)k * n + q] = sn * vkp + cs * vkq;
+          double *vk = v + (size_t)k * n;
+          const double vkp = vk[p], vkq = vk[q];
+          vk[p] = cs * vkp - sn * vkq;
+          vk[q] = sn * vkp + cs * vkq;
         }
       }
+    if (!rotated) break;
   }
+  auto at = [&](int i, int j) { return a[(size_t)i * n + j]; };
   std::vector<int> idx(n);
   for (int i = 0; i < n; i++) idx[i] = i;
-  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return at(x, x) < at(y, y); });
   std::vector<double> Vs((size_t)n * n);
   vals.resize(n);
   for (int j = 0; j < n; j++) {
-    vals[j] = a(idx[j], idx[j]);
+    vals[j] = at(idx[j], idx[j]);
     for (int i = 0; i < n; i++) Vs[(size_t)i * n + j] = V[(size_t)i * n + idx[j]];
   }
   V = Vs;
