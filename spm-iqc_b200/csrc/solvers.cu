@@ -304,8 +304,9 @@ int precond_many(spm_ctx *c, void *const *w, int n) {
 // coefficients B (k x k, row-major, B[p*k + q]) with X_new_q = sum_p B[p][q] X_p,
 // orthonormal for kept columns and zero for dropped ones.
 void gs_coefficients(const std::vector<double> &G, int k, double thr, std::vector<int> &keep,
-                     std::vector<double> &B) {
+                     std::vector<double> &B, std::vector<double> *pivots = nullptr) {
   std::vector<double> R((size_t)k * k, 0.0);
+  if (pivots) pivots->assign(k, 0.0);
   for (int j = 0; j < k; j++) {
     if (!keep[j]) continue;
     double r2 = G[(size_t)j * k + j];
@@ -322,6 +323,7 @@ void gs_coefficients(const std::vector<double> &G, int k, double thr, std::vecto
       continue;
     }
     R[(size_t)j * k + j] = std::sqrt(r2);
+    if (pivots) (*pivots)[j] = r2;
   }
   // B = R^{-1} on the kept index set (upper triangular back-substitution)
   B.assign((size_t)k * k, 0.0);
@@ -438,13 +440,18 @@ int orth_with_drop(spm_ctx *c, void *const *X, int k, double thr, std::vector<in
 
 // X (k fields) <- X orthogonalised against Q (nq orthonormal fields, zero
 // fields allowed) and among its own columns in order: block classical
-// Gram-Schmidt with a Cholesky factorisation of the Schur complement, two
-// passes of one Gram [Q X]^T X and one combination [Q X] -> X each (the
-// second re-orthogonalises). In the first pass a column whose norm after
-// projecting out Q and the columns before it is <= thr is dropped (zeroed,
-// keep[j] = 0): the 1e-8 tests of LOBPCG.cpp:298, 319, which follow the same
-// projections (Orthoi_v2V against V (and W), Orthoi_Vi against the earlier
-// columns) one column at a time.
+// Gram-Schmidt with a Cholesky factorisation of the Schur complement, one or
+// two passes of one Gram [Q X]^T X and one combination [Q X] -> X each. In the
+// first pass a column whose norm after projecting out Q and the columns before
+// it is <= thr is dropped (zeroed, keep[j] = 0): the 1e-8 tests of
+// LOBPCG.cpp:298, 319, which follow the same projections (Orthoi_v2V against V
+// (and W), Orthoi_Vi against the earlier columns) one column at a time. The
+// second pass re-orthogonalises, and is skipped when no column is dropped and
+// every column keeps at least half its squared norm through the projections
+// (its Cholesky pivot against its first-pass norm: "twice is enough", the
+// first pass is then orthogonal to working precision) -- the usual case for
+// the preconditioned residuals W, not for P (the previous block, nearly in the
+// span of the new one).
 int block_orth(spm_ctx *c, void *const *Q, int nq, void *const *X, int k, double thr, std::vector<int> &keep) {
   std::vector<void *> QX(Q, Q + nq);
   QX.insert(QX.end(), X, X + k);
@@ -458,7 +465,11 @@ int block_orth(spm_ctx *c, void *const *Q, int nq, void *const *X, int k, double
         for (int q = 0; q < nq; q++) v -= G[(size_t)q * k + i] * G[(size_t)q * k + j];
         S[(size_t)i * k + j] = v;
       }
-    gs_coefficients(S, k, pass == 0 ? thr : 0.0, keep, B);
+    std::vector<double> piv;
+    gs_coefficients(S, k, pass == 0 ? thr : 0.0, keep, B, &piv);
+    bool enough = pass == 0;
+    for (int j = 0; j < k && enough; j++)
+      enough = keep[j] && piv[j] >= 0.5 * G[(size_t)(nq + j) * k + j];
     // X_new = X B - Q (C B), C = Q^T X
     Cf.assign((size_t)m * k, 0.0);
     for (int q = 0; q < nq; q++)
@@ -470,6 +481,7 @@ int block_orth(spm_ctx *c, void *const *Q, int nq, void *const *X, int k, double
     for (int l = 0; l < k; l++)
       for (int j = 0; j < k; j++) Cf[(size_t)(nq + l) * k + j] = B[(size_t)l * k + j];
     SPM_TRY(combine(c, QX.data(), m, X, k, Cf, nullptr, false));
+    if (enough) break;
   }
   return SPM_OK;
 }
