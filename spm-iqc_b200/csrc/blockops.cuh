@@ -324,6 +324,13 @@ struct CombP {
   int chunk_bytes;                    // as GramP
   int stages;
   int *err;
+  // optional (staged kernel): norms[q] = inv_n sum_i Y_q[i]^2 of the outputs,
+  // summed in a fixed order through partials [grid][kBlkMax] and a ticket;
+  // norms[nout] receives the error word
+  double *norms;
+  double *partials;
+  unsigned *ticket;
+  double inv_n;
 };
 
 // Y_q[i] = (accumulate ? Y_q[i] : 0) + sum_p C[p][q] X_p[i] + d[q]. A point's
@@ -442,7 +449,11 @@ __global__ void __launch_bounds__((kCombWarps + 1) * 32, 1) combine_staged_kerne
                  &full[s]);
       if (lane == 0) s_issued = i + 1;
     }
-  } else {
+  }
+  double nsq[NO];  // squared norms of this thread's outputs
+#pragma unroll
+  for (int q = 0; q < NO; q++) nsq[q] = 0.0;
+  if (warp < kCombWarps) {
     const int grp = warp / kCombGroupWarps, gt = tid - grp * kCombGroupWarps * 32;
     for (int i = grp; i < mine; i += kCombWarps / kCombGroupWarps) {
       const int s = i % ST;
@@ -464,7 +475,11 @@ __global__ void __launch_bounds__((kCombWarps + 1) * 32, 1) combine_staged_kerne
         }
 #pragma unroll
         for (int q = 0; q < NO; q++)
-          if (q < p.nout) reinterpret_cast<T *>(p.Y[q])[base + j] = (T)(o[q] + p.d[q]);
+          if (q < p.nout) {
+            const T y = (T)(o[q] + p.d[q]);
+            reinterpret_cast<T *>(p.Y[q])[base + j] = y;
+            nsq[q] += (double)y * (double)y;
+          }
       }
       fence_proxy_async();
       __syncwarp();
@@ -485,6 +500,36 @@ __global__ void __launch_bounds__((kCombWarps + 1) * 32, 1) combine_staged_kerne
       mbar_inval(&full[s]);
       mbar_inval(&empty[s]);
     }
+  }
+  if (!p.norms) return;
+  // the outputs' squared norms: per CTA in a fixed thread order, then over
+  // the CTAs in a fixed order by the last CTA
+  __syncthreads();
+  double *red = reinterpret_cast<double *>(st);  // [threads][NO], over the idle ring
+  const int nthr = (kCombWarps + 1) * 32;
+#pragma unroll
+  for (int q = 0; q < NO; q++) red[(size_t)tid * NO + q] = nsq[q];
+  __syncthreads();
+  __shared__ int s_last;
+  if (tid < NO) {
+    double t = 0.0;
+    for (int u = 0; u < nthr; u++) t += red[(size_t)u * NO + tid];
+    p.partials[(size_t)blockIdx.x * kBlkMax + tid] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(p.ticket, 1u) == gridDim.x - 1u);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (tid < NO && tid < p.nout) {
+    double t = 0.0;
+    for (unsigned bk = 0; bk < gridDim.x; bk++) t += __ldcg(p.partials + (size_t)bk * kBlkMax + tid);
+    p.norms[tid] = t * p.inv_n;
+  }
+  if (tid == 0) {
+    p.norms[p.nout] = (double)*((volatile int *)p.err);
+    *p.ticket = 0u;
   }
 }
 

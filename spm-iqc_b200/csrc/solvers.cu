@@ -189,8 +189,11 @@ int gram(spm_ctx *c, void *const *X, int ma, void *const *Y, int mb, std::vector
 }
 
 // Y_q = (acc ? Y_q : 0) + sum_p C[p*nout + q] X_p + d[q]
+// norms (optional, host, nout entries): the outputs' squared norms under
+// inpfp, summed by the combination itself where it is staged (the call then
+// synchronises); on the other paths a Gram of the outputs supplies them.
 int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const std::vector<double> &C,
-            const std::vector<double> *d, bool acc) {
+            const std::vector<double> *d, bool acc, double *norms = nullptr) {
   if (nin > kBlkMax + 8 || nout > kBlkMax) return spm_fail(SPM_ERR_ARG, "combine size");
   CombP p;
   std::memset(&p, 0, sizeof(p));
@@ -229,7 +232,16 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
     if ((p.n * esz) % (size_t)p.chunk_bytes != 0)
       return spm_fail(SPM_ERR_ARG, "field size is not a whole number of combination chunks");
     p.err = c->flow + FW_ERR;
-    const size_t smem = (size_t)p.stages * nf * (p.chunk_bytes + 16) + 16 * (size_t)p.stages + 128;
+    Solver *sv = solver(c);
+    if (norms) {
+      p.norms = sv->gram_out;  // kBlkMax^2 + 8 doubles; the Gram buffers are idle between Grams
+      p.partials = sv->gram_part;
+      p.ticket = sv->gram_ticket;
+      p.inv_n = c->m.inv_n3;
+    }
+    const size_t ring = (size_t)p.stages * nf * (p.chunk_bytes + 16) + 16 * (size_t)p.stages;
+    const size_t red = norms ? sizeof(double) * 8 * (kCombWarps + 1) * 32 : 0;
+    const size_t smem = std::max(ring, red) + 128;
     auto launch_s = [&](auto kern) {
       e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramStagedSmemMax);
       if (e == cudaSuccess) kern<<<kStageBlocks, (kCombWarps + 1) * 32, smem, c->stream>>>(p);
@@ -241,7 +253,14 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
     if (nin <= 16) pick(combine_staged_kernel<double, 16, 8>, combine_staged_kernel<float, 16, 8>);
     else pick(combine_staged_kernel<double, kBlkMax + 8, 8>, combine_staged_kernel<float, kBlkMax + 8, 8>);
     if (e == cudaSuccess) e = cudaGetLastError();
-    return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "staged combine launch");
+    if (e != cudaSuccess) return spm_fail_cuda(e, "staged combine launch");
+    if (!norms) return SPM_OK;
+    e = cudaMemcpyAsync(sv->h_gram, sv->gram_out, sizeof(double) * (nout + 1), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return spm_fail_cuda(e, "combination norms");
+    if (sv->h_gram[nout] != 0.0) return spm_check_device_error(c);
+    std::copy(sv->h_gram, sv->h_gram + nout, norms);
+    return SPM_OK;
   }
   // register-bounded variants by block shape (two points per thread where they fit)
   auto launch = [&](auto kd, auto kf) {
@@ -253,7 +272,13 @@ int combine(spm_ctx *c, void *const *X, int nin, void *const *Y, int nout, const
   else if (nout <= 8) launch(combine_kernel<double, kBlkMax + 8, 8, 1>, combine_kernel<float, kBlkMax + 8, 8, 1>);
   else launch(combine_kernel<double, kBlkMax + 8, kBlkMax, 1>, combine_kernel<float, kBlkMax + 8, kBlkMax, 1>);
   e = cudaGetLastError();
-  return e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "combine launch");
+  if (e != cudaSuccess) return spm_fail_cuda(e, "combine launch");
+  if (norms) {
+    std::vector<double> G;
+    SPM_TRY(gram(c, Y, nout, Y, nout, G));
+    for (int q = 0; q < nout; q++) norms[q] = G[(size_t)q * nout + q];
+  }
+  return SPM_OK;
 }
 
 // Means of n fields (mean_Cplx, BasicOperators.cpp:121-130) into host memory.
@@ -600,10 +625,10 @@ static int lob_blocks(spm_ctx *c, void *V, int k, LobBlocks &B) {
 // W = U - alpha V and res_i = ||W_i||.
 static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::vector<double> &alpha,
                         std::vector<double> &res) {
-  std::vector<double> G;
   SPM_TRY(hv_many(c, phi, B.Vc.data(), B.U.data(), k));
-  SPM_TRY(gram(c, B.Vc.data(), k, B.U.data(), k, G));
-  for (int i = 0; i < k; i++) alpha[i] = G[(size_t)i * k + i];
+  // alpha_i = <V_i, H V_i>, summed by the Hessian product's epilogue
+  SPM_TRY(spm_read_scal(c, k));
+  for (int i = 0; i < k; i++) alpha[i] = c->host_scal[(size_t)i * kScal + SC_SUM1];
   {
     std::vector<void *> X(2 * k);
     std::vector<double> C((size_t)2 * k * k, 0.0);
@@ -613,10 +638,11 @@ static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::v
       C[(size_t)i * k + i] = 1.0;
       C[(size_t)(k + i) * k + i] = -alpha[i];
     }
-    SPM_TRY(combine(c, X.data(), 2 * k, B.W.data(), k, C, nullptr, false));
+    // res_i = ||W_i||, summed by the combination that forms W
+    std::vector<double> nrm(k);
+    SPM_TRY(combine(c, X.data(), 2 * k, B.W.data(), k, C, nullptr, false, nrm.data()));
+    for (int i = 0; i < k; i++) res[i] = std::sqrt(std::max(0.0, nrm[i]));
   }
-  SPM_TRY(gram(c, B.W.data(), k, B.W.data(), k, G));
-  for (int i = 0; i < k; i++) res[i] = std::sqrt(std::max(0.0, G[(size_t)i * k + i]));
   return SPM_OK;
 }
 
