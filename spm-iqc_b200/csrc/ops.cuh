@@ -394,23 +394,44 @@ template <class T> struct EpiNgrad {
 
 // hv_cam epilogue (LOBPCG.cpp:136-156): y + (-Tau - 2 Gamma phi + 3 phi^2) v - mu.
 // aux0 = phi, aux1 = v.
-// Also sums v (H v): scal[SC_SUM1] = <v, H v>, the Rayleigh quotient LOBPCG
-// takes for each vector of its block (LOBPCG.cpp:270-286) without a Gram pass.
-template <class T> struct EpiHv {
-  static constexpr int NR = 1;
+// The Hessian product before its mean removal, for LOBPCG's block: o = y +
+// (-Tau - 2 Gamma phi + 3 phi^2) v, whose mean is the mu that hv_cam subtracts
+// (LOBPCG.cpp:136-156). Sums scal[SC_MU] = mean(o), scal[SC_SUM1] = <v, o>,
+// scal[SC_SUM2] = mean(v), so the caller can apply the projection where it uses
+// the product (no pass over phi before the transform). aux0 = phi, aux1 = v.
+template <class T> struct EpiHvRaw {
+  static constexpr int NR = 3;
   static constexpr unsigned MAXM = 0;
-  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&acc)[1]) {
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&acc)[3]) {
+    const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
+    const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
+    const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma;
+    const c2<T> o = {y.x + (-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * v.x,
+                     y.y + (-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * v.y};
+    acc[0] += (double)o.x + (double)o.y;
+    acc[1] += (double)v.x * (double)o.x + (double)v.y * (double)o.y;
+    acc[2] += (double)v.x + (double)v.y;
+    return o;
+  }
+  __device__ static void fin(const KParams &p, int b, const double (&tot)[3]) {
+    double *sc = scal_of(p, b);
+    sc[SC_MU] = tot[0] * p.m.inv_n3;
+    sc[SC_SUM1] = tot[1] * p.m.inv_n3;
+    sc[SC_SUM2] = tot[2] * p.m.inv_n3;
+  }
+};
+
+template <class T> struct EpiHv {
+  static constexpr int NR = 0;
+  static constexpr unsigned MAXM = 0;
+  __device__ static c2<T> epi(const KParams &p, int b, size_t idx, c2<T> y, double (&)[1]) {
     const c2<T> ph = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux0[b]) + idx));
     const c2<T> v = __ldg(reinterpret_cast<const c2<T> *>(fld<T>(p.aux1[b]) + idx));
     const T tau = (T)p.m.Tau, gam = (T)p.m.Gamma, mu = (T)scal_of(p, b)[SC_MU];
-    const c2<T> o = {y.x + (-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * v.x - mu,
-                     y.y + (-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * v.y - mu};
-    acc[0] += (double)v.x * (double)o.x + (double)v.y * (double)o.y;
-    return o;
+    return c2<T>{y.x + (-tau - (T)2 * gam * ph.x + (T)3 * ph.x * ph.x) * v.x - mu,
+                 y.y + (-tau - (T)2 * gam * ph.y + (T)3 * ph.y * ph.y) * v.y - mu};
   }
-  __device__ static void fin(const KParams &p, int b, const double (&tot)[1]) {
-    scal_of(p, b)[SC_SUM1] = tot[0] * p.m.inv_n3;
-  }
+  __device__ static void fin(const KParams &, int, const double (&)[1]) {}
 };
 
 // Tangent epilogue: returns Gv and, when p.sto[b] is set, also writes the

@@ -498,6 +498,26 @@ template <int N, class T> struct Impl {
     return plane_inv<N, T, EpiHv<T>>(c, r, n);
   }
 
+  // n <= kMaxBatch Hessian products without their mean removal (EpiHvRaw):
+  // v is transformed as it is, so phi is read once, by the epilogue.
+  static int hv_raw(spm_ctx *c, const void *phi, const void *const *v, void *const *hv, int n) {
+    SPM_NEED_SCRATCH(c, n);
+    KParams p = spm_params(c), q = spm_params(c), r = spm_params(c);
+    for (int b = 0; b < n; b++) {
+      p.in[b] = v[b];
+      p.out[b] = spm_bufA(c, b);
+      q.in[b] = spm_bufA(c, b);
+      q.out[b] = spm_bufB(c, b);
+      r.in[b] = spm_bufB(c, b);
+      r.aux0[b] = phi;
+      r.aux1[b] = v[b];
+      r.out[b] = hv[b];
+    }
+    SPM_TRY((plane_fwd<N, T, ProIdent<T>>(c, p, n)));
+    SPM_TRY((pencil<N, T, OpGmul<T, false>>(c, q, n)));
+    return plane_inv<N, T, EpiHvRaw<T>>(c, r, n);
+  }
+
   // n <= kMaxBatch preconditioner applications, in place.
   static int precond(spm_ctx *c, void *const *w, int n) {
     SPM_NEED_SCRATCH(c, n);
@@ -614,7 +634,7 @@ template <int N, class T> struct Impl {
 
   static const OpsTable *table() {
     static const OpsTable t = {&fft, &ifft, &energy, &grad_step, &grad_steps, &grad_steps_ev, &grad_step_ev, &ngrad, &hv, &precond, &dot,
-                               &tangent, &force, &gnorm, &hisd_step, &grad_steps_group};
+                               &tangent, &force, &gnorm, &hisd_step, &grad_steps_group, &hv_raw};
     return &t;
   }
 };

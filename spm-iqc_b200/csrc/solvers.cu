@@ -302,12 +302,28 @@ int means(spm_ctx *c, void *const *X, int n, std::vector<double> &out) {
   return SPM_OK;
 }
 
-int hv_many(spm_ctx *c, const void *phi, void *const *v, void *const *hv, int n) {
+// The LOBPCG block's Hessian products (hv_cam, LOBPCG.cpp:113-166) without
+// their final mean removal: hv[b] = H v_b + mu_b, mu_b the constant hv_cam
+// subtracts. The block uses them where that constant cancels or is applied
+// exactly: the Rayleigh-Ritz Gram against mean-free vectors, and the residual
+// combination W = H V - alpha V, which subtracts mu. With mu / vhv (host, n
+// entries) the call returns mu_b and <v_b, H v_b> (after the mean removal) and
+// synchronises.
+int hv_many(spm_ctx *c, const void *phi, void *const *v, void *const *hv, int n, double *mu = nullptr,
+            double *vhv = nullptr) {
   const OpsTable *t = spm_table_of(c);
   for (int b0 = 0; b0 < n; b0 += kMaxBatch) {
     const int nb = std::min(kMaxBatch, n - b0);
     SPM_TRY(spm_ensure_scratch(c, nb));
-    SPM_TRY(t->hv(c, phi, (const void *const *)(v + b0), hv + b0, nb));
+    SPM_TRY(t->hv_raw(c, phi, (const void *const *)(v + b0), hv + b0, nb));
+    if (mu || vhv) {
+      SPM_TRY(spm_read_scal(c, nb));
+      for (int b = 0; b < nb; b++) {
+        const double *sc = c->host_scal + (size_t)b * kScal;
+        if (mu) mu[b0 + b] = sc[SC_MU];
+        if (vhv) vhv[b0 + b] = sc[SC_SUM1] - sc[SC_MU] * sc[SC_SUM2];
+      }
+    }
   }
   return SPM_OK;
 }
@@ -621,26 +637,28 @@ static int lob_blocks(spm_ctx *c, void *V, int k, LobBlocks &B) {
   return SPM_OK;
 }
 
-// First half of an iteration (LOBPCG.cpp:270-286): U = H V, alpha = <V, U>,
-// W = U - alpha V and res_i = ||W_i||.
+// First half of an iteration (LOBPCG.cpp:270-286): U = H V (kept before its
+// mean removal, see hv_many), alpha = <V, H V>, W = H V - alpha V and
+// res_i = ||W_i||.
 static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::vector<double> &alpha,
                         std::vector<double> &res) {
-  SPM_TRY(hv_many(c, phi, B.Vc.data(), B.U.data(), k));
-  // alpha_i = <V_i, H V_i>, summed by the Hessian product's epilogue
-  SPM_TRY(spm_read_scal(c, k));
-  for (int i = 0; i < k; i++) alpha[i] = c->host_scal[(size_t)i * kScal + SC_SUM1];
+  // U = H V + mu (the Hessian products before their mean removal); alpha_i =
+  // <V_i, H V_i> and mu_i summed by the products' epilogue
+  std::vector<double> mu(k);
+  SPM_TRY(hv_many(c, phi, B.Vc.data(), B.U.data(), k, mu.data(), alpha.data()));
   {
     std::vector<void *> X(2 * k);
-    std::vector<double> C((size_t)2 * k * k, 0.0);
+    std::vector<double> C((size_t)2 * k * k, 0.0), d(k);
     for (int i = 0; i < k; i++) {
       X[i] = B.U[i];
       X[k + i] = B.Vc[i];
       C[(size_t)i * k + i] = 1.0;
       C[(size_t)(k + i) * k + i] = -alpha[i];
+      d[i] = -mu[i];
     }
-    // res_i = ||W_i||, summed by the combination that forms W
+    // W = H V - alpha V; res_i = ||W_i||, summed by the combination that forms W
     std::vector<double> nrm(k);
-    SPM_TRY(combine(c, X.data(), 2 * k, B.W.data(), k, C, nullptr, false, nrm.data()));
+    SPM_TRY(combine(c, X.data(), 2 * k, B.W.data(), k, C, &d, false, nrm.data()));
     for (int i = 0; i < k; i++) res[i] = std::sqrt(std::max(0.0, nrm[i]));
   }
   return SPM_OK;
@@ -649,7 +667,10 @@ static int lob_residual(spm_ctx *c, const void *phi, LobBlocks &B, int k, std::v
 // Second half (LOBPCG.cpp:287-449): W = P0(precond(W)) perp V with
 // Gram-Schmidt and the 1e-8 dropping, Y = H W; P perp [V, W], dropping,
 // Up = H P; Rayleigh-Ritz on [V; W; P]; P <- V; V <- the k lowest Ritz
-// vectors, mean removed and Gram-Schmidt orthonormalised.
+// vectors, mean removed and Gram-Schmidt orthonormalised. The products U, Y,
+// Up carry the constant that hv_cam's mean removal subtracts (hv_many); the
+// Rayleigh-Ritz Gram pairs them with the mean-free V, W, P, where a constant
+// adds nothing.
 // With V0 (k0 fixed orthonormal fields, GOSD.cpp) W, P and the new V are also
 // kept orthogonal to V0.
 static int lob_update(spm_ctx *c, const void *phi, LobBlocks &B, int k, bool &have_p, void *const *V0 = nullptr,

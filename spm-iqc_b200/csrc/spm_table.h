@@ -23,6 +23,8 @@ struct OpsTable {
   int (*hisd_step)(spm_ctx *, void *x, const void *t, void *dx, double beta);
   // K gated steps of n instances of one grid size and precision, one launch per pass for all
   int (*grad_steps_group)(spm_ctx *const *ctx, void *const *phi, void *const *uhat, int n, int nsteps);
+  // Hessian products before their mean removal; scal: SC_MU = the mean, SC_SUM1 = <v, o>, SC_SUM2 = mean(v)
+  int (*hv_raw)(spm_ctx *, const void *phi, const void *const *v, void *const *hv, int n);
 };
 
 // prec: 0 = FP64, 1 = FP32
