@@ -406,10 +406,11 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
 // groups of 8 consumer warps (alternate chunks, so two chunks are worked on at
 // once) computes the chunk's outputs point by point (thread j of the
 // chunk: Y_q[j] = sum_p C[p][q] X_p[j] + d[q], the coefficients read from the
-// kernel parameters at fixed offsets) and store them. Same operations in the
+// kernel parameters at fixed offsets) and stores them. Same operations in the
 // same order as combine_kernel, so the results are the same bits. A chunk's
 // inputs are all in shared memory before any of its outputs is stored, and
-// chunks are disjoint, so Y may alias X.
+// chunks are disjoint, so Y may alias X. With p.norms the kernel also returns
+// the outputs' squared norms (LOBPCG's residual norms of W = H V - alpha V).
 constexpr int kCombWarps = 16;  // consumer warps: two groups of 8, taking alternate chunks
 constexpr int kCombGroupWarps = 8;
 template <class T, int NI, int NO>
