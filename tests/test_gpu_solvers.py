@@ -61,6 +61,31 @@ def test_lobpcg_matches_oracle(spm, cuda, N, k, iters):
     assert np.max(np.abs(Vg.reshape(k, -1).mean(1))) < 1e-14
 
 
+@pytest.mark.parametrize("k", [8, 3])
+def test_lobpcg_direct_block_kernels_agree(spm, cuda, k):
+    """The block kernels staged through shared memory (default) and the direct
+    ones (knob block_stage 0: Grams by gram_kernel, the residual norms from a
+    Gram of W instead of the combination) give the same LOBPCG iterates to
+    rounding; k = 3 runs the residual combination on the direct kernel even
+    when staged (six inputs)."""
+    N = 64
+    m = npo.Model(N)
+    phi = t(cuda, npo.uniform_field(N, 7))
+    V0 = m.lobpcg_init(k, 5)
+    out = []
+    for stage in (1, 0):
+        ctx = spm.SpmContext(N)
+        ctx.tune("block_stage", stage)
+        Vd = t(cuda, V0)
+        ev, rs, it = ctx.hiosd_lobpcg_inip(phi, Vd, 10)
+        out.append((ev, rs, Vd.cpu().numpy()))
+    (e1, r1, V1), (e0, r0, V0b) = out
+    assert np.max(np.abs(e1 - e0)) <= 1e-12 * np.max(np.abs(e0))
+    assert np.max(np.abs(r1 - r0)) <= 1e-9 * np.max(r0)
+    s = np.linalg.svd(V1.reshape(k, -1) @ V0b.reshape(k, -1).T / N ** 3, compute_uv=False)
+    assert np.min(s) > 1 - 1e-10
+
+
 def test_lobpcg_at_zero_field_finds_lowest_kernel_modes(spm, cuda):
     """Known answer: H(0) is diagonal in k with eigenvalues G(k) - Tau. With
     L = 5 on a 32^3 grid the |n| = 5 shell (30 modes, k^2 = 1, G = min) is an
