@@ -516,8 +516,8 @@ def config_legs(ctx, phi_h):
     config3: Spring_Pairing (SPM.cpp:170-263) from that stationary point +- delta v1
       (v1 the unstable eigenmode, nrmp(v1) = 1; delta = 0.001, the reference's
       own separation, main_SPM.cpp:109-119) in FP64 and in FP32 + FP64 polish,
-      with the saddle energy and the unstable eigenvalue (LOBPCG k = 2 at the
-      saddle) of the mixed run against the all-FP64 run."""
+      with the saddle energy and the unstable eigenvalue (LOBPCG k = 1 with 3
+      guard vectors at the saddle) of the mixed run against the all-FP64 run."""
     import numpy as np
     import torch
     out = {"config2": {}, "config3": {}}
@@ -575,12 +575,14 @@ def config_legs(ctx, phi_h):
             (h, n32, n64), sec = timed(lambda: ctx.Spring_Pairing_mixed(p0, p1, cap3, tol3, switch_tol=sw3))
         mid = (0.5 * (p0 + p1)).contiguous()
         um = ctx.my_fft(mid)
-        W = ctx.hiosd_lobpcg_initialization(2, seed=9)
-        ev, rs, lits = ctx.hiosd_lobpcg_inip(mid, W, maxiter=800, tol=1e-8)
+        # the unstable mode: LOBPCG k = 1 with 3 guard vectors (the translation
+        # modes, eigenvalues ~1e-8, sit close above it)
+        W = ctx.hiosd_lobpcg_initialization(4, seed=9)
+        ev, rs, lits = ctx.lobpcg_guarded(mid, W, 1, maxiter=800, tol=1e-8)
         c3[mode] = {"seconds": sec, "fp32_iterations": n32, "fp64_iterations": n64, "residual": float(h[-1]),
                     "reached": bool(h[-1] <= tol3), "saddle_energy": ctx.get_Ene(mid, um),
-                    "unstable_eigenvalue": float(ev[0]), "lobpcg_iterations": lits,
-                    "lobpcg_residual": float(max(rs))}
+                    "unstable_eigenvalue": float(ev[0]), "lobpcg_k": 1, "lobpcg_guard": 3,
+                    "lobpcg_iterations": lits, "lobpcg_residual": float(rs[0])}
         del p0, p1, mid, um, W
         torch.cuda.empty_cache()
     c3["mixed"]["switch_tol"] = sw3
