@@ -234,12 +234,15 @@ extern "C" int spm_selftest_bounded_wait(spm_ctx *c, int polls) {
 }
 
 int spm_read_scal(spm_ctx *c, int nb) {
+  // the scalars and the error word of the bounded waits in one round trip
   cudaError_t e = cudaMemcpyAsync(c->host_scal, c->scal, sizeof(double) * kScal * nb, cudaMemcpyDeviceToHost,
                                   c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->host_flow + FW_ERR, c->flow + FW_ERR, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "scalar read");
   e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return spm_fail_cuda(e, "stream sync");
-  return spm_check_device_error(c);
+  return c->host_flow[FW_ERR] ? spm_check_device_error(c) : SPM_OK;
 }
 
 extern "C" int spm_ctx_create(int N, double L, double Tau, double Gamma, double dt, int precision, void *stream,
