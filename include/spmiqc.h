@@ -312,7 +312,8 @@ int spm_block_gram(spm_ctx *ctx, const void *const *X, int ma, const void *const
  * <= 32, 1 <= nout <= 24; X, Y host arrays of device field pointers; C a host
  * array of nin*nout doubles, d of nout doubles or NULL for zeros). A point's
  * inputs are all read before any of its outputs is written, so Y may alias X
- * (an in-place update). Enqueued on the context's stream. */
+ * (an in-place update); a field may not appear twice in Y (SPM_ERR_ARG).
+ * Enqueued on the context's stream. */
 int spm_block_combine(spm_ctx *ctx, const void *const *X, int nin, void *const *Y, int nout, const double *C,
                       const double *d);
 

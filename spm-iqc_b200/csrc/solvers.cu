@@ -575,8 +575,11 @@ extern "C" int spm_block_combine(spm_ctx *c, const void *const *X, int nin, void
     return spm_fail(SPM_ERR_ARG, "bad argument (1 <= nin <= 32, 1 <= nout <= 24)");
   for (int i = 0; i < nin; i++)
     if (!X[i]) return spm_fail(SPM_ERR_ARG, "null field in X");
-  for (int i = 0; i < nout; i++)
+  for (int i = 0; i < nout; i++) {
     if (!Y[i]) return spm_fail(SPM_ERR_ARG, "null field in Y");
+    for (int j = 0; j < i; j++)
+      if (Y[j] == Y[i]) return spm_fail(SPM_ERR_ARG, "a field appears twice in Y");
+  }
   const std::vector<double> Cv(C, C + (size_t)nin * nout);
   std::vector<double> dv;
   if (d) dv.assign(d, d + nout);

@@ -205,6 +205,19 @@ def test_block_combine(spm, cuda, N, prec, shape):
     assert np.array_equal(outs[0], outs[1])
 
 
+def test_block_entry_points_reject_bad_blocks(spm, cuda):
+    """spm_block_gram / spm_block_combine refuse blocks beyond their limits and
+    an output field listed twice."""
+    ctx = spm.SpmContext(32)
+    f = ctx.field(3)
+    with pytest.raises(spm.SpmError):
+        ctx.block_gram([f[0]] * 25, [f[1]])
+    with pytest.raises(spm.SpmError):
+        ctx.block_combine([f[0], f[1]], [f[2], f[2]], np.ones((2, 2)))
+    with pytest.raises(spm.SpmError):
+        ctx.block_combine([f[0]] * 33, [f[1]], np.ones((33, 1)))
+
+
 @pytest.mark.parametrize("N", [32, 64, 128, 160, 192])
 def test_fused_plane_chain_is_bit_identical(spm, cuda, N):
     """Chains of steps with the fused inverse -> forward plane pass give the
