@@ -689,6 +689,8 @@ def main():
     ap.add_argument("--schedule", default=None,
                     help="plane_cps,fuse_planes,plane_xg for the FP64 context instead of the autotuner's choice "
                          "(fixed kernel variants for ncu captures)")
+    ap.add_argument("--tune", action="append", default=[], metavar="KNOB=V",
+                    help="set a tuning knob (spm_tune) of the flow contexts before the autotuner runs, e.g. pdl=0")
     ap.add_argument("--serve", action="store_true", help="run the serving workload instead (one JSON line)")
     ap.add_argument("--serve-jobs", type=int, default=40)
     ap.add_argument("--serve-jobs-default", type=int, default=32,
@@ -727,6 +729,9 @@ def main():
     # --only-flow may time the flow in FP32 (for captures of the FP32 kernels)
     prec = args.flow_precision if args.only_flow else "fp64"
     ctx = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, prec, stream=stream.cuda_stream)
+    knobs = [(kv.split("=")[0], int(kv.split("=")[1])) for kv in args.tune]
+    for knob, v in knobs:
+        ctx.tune(knob, v)
     # schedule choice by the autotuner, outside the timed region (FP32 too, for
     # the FP32 leg and the FP32 twin of the mixed flow)
     if args.schedule:
@@ -736,6 +741,8 @@ def main():
         ctx.autotune(60)
     sched64 = ctx.tuning()
     _c32 = spmiqc.SpmContext(N, L, TAU, GAMMA, DT, "fp32", stream=stream.cuda_stream)
+    for knob, v in knobs:
+        _c32.tune(knob, v)
     if not args.schedule:
         _c32.autotune(60)
     sched32 = _c32.tuning()

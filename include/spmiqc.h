@@ -107,14 +107,20 @@ const char *spm_status_str(int status);
  * knob "block_stage" (1 or 0): the LOBPCG block kernels (Grams, combinations
  * of more than 8 fields) stage their fields through shared memory with bulk
  * copies (1) or load them directly (0).
+ * knob "pdl" (0 or 1): 1 = the plane and pencil kernels are launched as
+ * programmatic dependents (not while the stream is being captured into a
+ * graph): a launch may be set up while the previous kernel of the stream
+ * completes, and its kernel waits on the device for that kernel before its
+ * first memory access; 0 (default) = plain stream order. The same bits
+ * either way; spm_autotune turns it on where it is at least 1 % faster.
  * spm_tune_get returns the current value or -1 for an unknown knob. */
 int spm_tune(spm_ctx *ctx, const char *knob, int value);
 int spm_tune_get(const spm_ctx *ctx, const char *knob);
 /* Autotuner (no counterpart in the reference): times chains of `steps`
  * gradient steps on a scratch field for each candidate schedule (plane_cps
  * 1/2/3 with fused chains, plane_cps 2 without, plane_xg 1/2/3 with plane_cps
- * 2 and 3 on fused chains, plane_cps 4 for FP32, 5, 6; then pencil_tc 4 for the
- * best of them), keeping a later candidate only if it is at least 1 % faster, and
+ * 2 and 3 on fused chains, plane_cps 4 for FP32, 5, 6; then pencil_tc 4 and
+ * pdl 1 for the best of them), keeping a later candidate only if it is at least 1 % faster, and
  * keeps the fastest in the context; the choice is remembered per (device, N, precision), so later
  * contexts of the same kind take it without timing (FP32 twins of mixed flows
  * included). Synchronises; allocates two scratch fields while it runs. The

@@ -4,7 +4,8 @@
 // with two CTAs per SM, or three CTAs per SM with fewer registers per thread),
 // whether gradient chains use the fused inverse -> forward plane pass, and
 // whether their plane kernels exchange through distributed shared memory or
-// through global areas resident in L2.
+// through global areas resident in L2; then, for the fastest, the pencil tile
+// width and programmatic dependent launches (knob "pdl").
 // Each candidate runs a short chain of gradient steps on a scratch field with
 // CUDA events around it; the fastest is kept in the context and remembered per
 // (device, N, precision) for later contexts.
@@ -22,7 +23,7 @@ namespace {
 
 std::mutex g_mu;
 struct Choice {
-  int plane_cps, fuse_planes, plane_xg, pencil_tc = 8;
+  int plane_cps, fuse_planes, plane_xg, pencil_tc = 8, pdl = 0;
 };
 std::map<std::tuple<int, int, int>, Choice> g_best;  // (device, N, prec) -> schedule
 
@@ -41,7 +42,7 @@ template <class T> __global__ void fill_kernel(T *phi, int N) {
 
 // The remembered choice for (device, N, precision), if any.
 bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg,
-                         int *pencil_tc) {
+                         int *pencil_tc, int *pdl) {
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_best.find(std::make_tuple(device, N, prec));
   if (it == g_best.end()) return false;
@@ -49,6 +50,7 @@ bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_
   *fuse_planes = it->second.fuse_planes;
   *plane_xg = it->second.plane_xg;
   if (pencil_tc) *pencil_tc = it->second.pencil_tc;
+  if (pdl) *pdl = it->second.pdl;
   return true;
 }
 
@@ -60,6 +62,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
     c->fuse_planes = ch.fuse_planes;
     c->plane_xg = ch.plane_xg;
     c->pencil_tc = ch.pencil_tc;
+    c->pdl = ch.pdl;
     if (!c->plane_xg && c->xg) {  // the exchange areas are not used by the chosen schedule
       cudaStreamSynchronize(c->stream);
       cudaFree(c->xg);
@@ -85,7 +88,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   int rc = e == cudaSuccess ? SPM_OK : spm_fail_cuda(e, "autotune buffers");
-  const Choice saved = {c->plane_cps, c->fuse_planes, c->plane_xg, c->pencil_tc};
+  const Choice saved = {c->plane_cps, c->fuse_planes, c->plane_xg, c->pencil_tc, c->pdl};
   Choice best = saved;
   float best_ms = 1e30f;
   // plane variant, fused plane pass, exchange routes of the gradient chains
@@ -101,6 +104,7 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
     c->fuse_planes = cand.fuse_planes;
     c->plane_xg = cand.plane_xg;
     c->pencil_tc = cand.pencil_tc;
+    c->pdl = cand.pdl;
     int r = spm_ensure_xg(c);
     if (r != SPM_OK) return r;
     if (c->prec == SPM_FP64) fill_kernel<double><<<592, 256, 0, c->stream>>>((double *)phi, c->N);
@@ -141,6 +145,18 @@ extern "C" int spm_autotune(spm_ctx *c, int steps, int *plane_cps, int *fuse_pla
     if (rc == SPM_OK && t < 0.99f * best_ms) {
       best_ms = t;
       best = narrow;
+    }
+  }
+  // and programmatic dependent launches of the plane and pencil kernels, if
+  // they are at least 1 % faster
+  if (rc == SPM_OK) {
+    Choice dep = best;
+    dep.pdl = 1;
+    float t = 1e30f;
+    rc = time_it(dep, t);
+    if (rc == SPM_OK && t < 0.99f * best_ms) {
+      best_ms = t;
+      best = dep;
     }
   }
   if (e0) cudaEventDestroy(e0);

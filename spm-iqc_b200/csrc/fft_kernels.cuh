@@ -478,6 +478,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_fwd_kernel(const __grid_con
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
+  grid_dep_sync();
   if (flow_stopped(p, blockIdx.y)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
@@ -587,6 +588,7 @@ __global__ void __launch_bounds__(PencilGeo<N, TC>::TH,
   double *red = reinterpret_cast<double *>(bars + 2);
   double2 *stab = reinterpret_cast<double2 *>(red + 32 * kRedMax);  // symbol buffers (one or two tiles)
   __shared__ int s_err;
+  grid_dep_sync();
   if (flow_stopped(p, blockIdx.y)) return;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -839,6 +841,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_kernel(const __grid_con
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (STAGED ? G::STAGE_UNITS : 0));
   double *red = reinterpret_cast<double *>(bar + 2);
   __shared__ int s_err;
+  grid_dep_sync();
   if (flow_stopped(p, blockIdx.y)) return;
 
   cg::cluster_group cluster = cg::this_cluster();
@@ -936,6 +939,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_kernel(const __grid
   T2 *buf = ztw + N / 2;
   uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
   double *red = reinterpret_cast<double *>(bar + 2);
+  grid_dep_sync();
   if (flow_stopped(p, blockIdx.y)) return;
   // uniform over the grid: set by the pencil pass of this step, before launch
   const bool stop = flow_pending(p, blockIdx.y);
@@ -1062,6 +1066,7 @@ __global__ void __launch_bounds__(8 * RW, CPS) plane_inv_fwd_pipe_kernel(const _
   T2 *buf = ztw + N / 2;
   uint64_t *bar = reinterpret_cast<uint64_t *>(buf + P::UNITS);
   double *red = reinterpret_cast<double *>(bar + 2);
+  grid_dep_sync();
   if (flow_stopped(p, blockIdx.y)) return;
   const bool stop = flow_pending(p, blockIdx.y);
 

@@ -31,8 +31,19 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
   return e;
 }
 
+// Programmatic dependent launches (knob "pdl") on a stream that is not being
+// captured into a graph (captures keep plain stream order).
+static inline bool pdl_on(const spm_ctx *c) {
+  if (!c->pdl) return false;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(c->stream, &st) == cudaSuccess && st == cudaStreamCaptureStatusNone;
+}
+
 // Persistent cluster launch: as many clusters as can be resident at once
-// (queried once per kernel and device), at most one per x-plane.
+// (queried once per kernel and device), at most one per x-plane. With
+// pdl_on the launch is a programmatic dependent one: its CTAs may be placed
+// while the previous kernel of the stream finishes, and wait for it in
+// grid_dep_sync.
 template <class Tag, int N, class K, int RW = kRows>
 static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int nb, const char *what,
                           bool xg = false, int regions = 2) {
@@ -51,11 +62,13 @@ static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int
   cfg.blockDim = dim3(8 * RW, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = c->stream;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = CLr;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
   // the grid depends only on the kernel and the device (never on the load),
@@ -72,6 +85,7 @@ static int launch_cluster(spm_ctx *c, K kern, size_t smem, const KParams &p, int
     ncl[dev].store(nc, std::memory_order_relaxed);
   }
   cfg.gridDim = dim3(CLr * nc, nb, 1);
+  cfg.numAttrs = pdl_on(c) ? 2 : 1;  // the kernels begin with grid_dep_sync
   // a kernel exchanging through global areas needs one per CTA (nb == 1)
   if (xg && (!p.xg || nb != 1 || CLr * nc > p.xg_cap * (kRows / RW) || p.xg_regions < regions))
     return spm_fail(SPM_ERR_STATE, "plane exchange areas missing or too small");
@@ -217,7 +231,7 @@ template <int N, class T, class Epi, class Pro> static int plane_inv_fwd(spm_ctx
   return plane_inv_fwd_xg<N, T, Epi, Pro, 0>(c, p, nb);
 }
 // Persistent pencil launch: resident CTAs (queried once), at most one per tile;
-// tiles of 8 columns, or 4 (knob "pencil_tc").
+// tiles of 8 columns, or 4 (knob "pencil_tc"); programmatic dependent with pdl_on.
 template <int N, class T, class Op, int TC> static int pencil_tc(spm_ctx *c, const KParams &p0, int nb) {
   using PG = PencilGeo<N, TC>;
   KParams p = p0;
@@ -244,9 +258,18 @@ template <int N, class T, class Op, int TC> static int pencil_tc(spm_ctx *c, con
     nbk = per_sm * sms < PG::PTILES ? per_sm * sms : PG::PTILES;
     nblk[dev].store(nbk, std::memory_order_relaxed);
   }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nbk, nb, 1);
+  cfg.blockDim = dim3(PG::TH, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_on(c) ? 1 : 0;  // the kernel begins with grid_dep_sync
   c->launches++;
-  kern<<<dim3(nbk, nb, 1), PG::TH, smem, c->stream>>>(p);
-  e = cudaGetLastError();
+  e = cudaLaunchKernelEx(&cfg, kern, p);
   return e == cudaSuccess ? 0 : spm_fail_cuda(e, "pencil launch");
 }
 template <int N, class T, class Op> static int pencil(spm_ctx *c, const KParams &p, int nb) {

@@ -397,6 +397,11 @@ extern "C" int spm_tune(spm_ctx *c, const char *knob, int value) {
     c->block_stage = value;
     return SPM_OK;
   }
+  if (std::strcmp(knob, "pdl") == 0) {
+    if (value != 0 && value != 1) return spm_fail(SPM_ERR_ARG, "pdl must be 0 or 1");
+    c->pdl = value;
+    return SPM_OK;
+  }
   return spm_fail(SPM_ERR_ARG, "unknown tuning knob");
 }
 
@@ -408,6 +413,7 @@ extern "C" int spm_tune_get(const spm_ctx *c, const char *knob) {
   if (std::strcmp(knob, "batch_group") == 0) return c->batch_group;
   if (std::strcmp(knob, "pencil_tc") == 0) return c->pencil_tc;
   if (std::strcmp(knob, "block_stage") == 0) return c->block_stage;
+  if (std::strcmp(knob, "pdl") == 0) return c->pdl;
   return -1;
 }
 
@@ -600,10 +606,11 @@ int spm_ensure_twin(spm_ctx *c) {
   c->twin->batch_group = c->batch_group;
   c->twin->pencil_tc = c->pencil_tc;
   c->twin->block_stage = c->block_stage;
+  c->twin->pdl = c->pdl;
   c->twin->spring_len = c->spring_len;
   // an FP32 schedule chosen by spm_autotune on an FP32 context of this size wins
   spm_autotune_lookup(c->device, c->N, SPM_FP32, &c->twin->plane_cps, &c->twin->fuse_planes, &c->twin->plane_xg,
-                      &c->twin->pencil_tc);
+                      &c->twin->pencil_tc, &c->twin->pdl);
   return spm_ensure_xg(c->twin);
 }
 

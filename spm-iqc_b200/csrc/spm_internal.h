@@ -57,6 +57,7 @@ struct spm_ctx {
   int batch_group = 1;          // spm_batch_grad_flow: same-size instances share launches (knob "batch_group")
   int pencil_tc = 8;            // pencil tile width in complex columns: 8 or 4 (knob "pencil_tc")
   int block_stage = 1;          // solver Grams stage their fields through shared memory (knob "block_stage")
+  int pdl = 0;                  // plane and pencil kernels launched as programmatic dependents (knob "pdl")
   double spring_len = 0.0;      // SPM spring rest length (0: the reference's zero-length spring)
   spm_ctx *twin = nullptr;      // FP32 twin of an FP64 context (mixed-precision flows)
   void *twin_buf = nullptr;     // FP32 phi and uhat of the twin
@@ -95,5 +96,5 @@ struct FloorWatch {
 
 // The autotuner's remembered choice for (device, N, precision), if any.
 bool spm_autotune_lookup(int device, int N, int prec, int *plane_cps, int *fuse_planes, int *plane_xg,
-                         int *pencil_tc = nullptr);
+                         int *pencil_tc = nullptr, int *pdl = nullptr);
 const struct OpsTable *spm_table_of(const spm_ctx *c);

@@ -251,7 +251,7 @@ class SpmContext:
         """The current values of the tuning knobs (spm_tune_get)."""
         f = lib().spm_tune_get
         f.argtypes = [_vp, ctypes.c_char_p]
-        return {k: int(f(self.h, k.encode())) for k in ("plane_cps", "fuse_planes", "plane_xg", "pencil_tc")}
+        return {k: int(f(self.h, k.encode())) for k in ("plane_cps", "fuse_planes", "plane_xg", "pencil_tc", "pdl")}
 
     def ngrad_cam(self, phi, grad=None):
         grad = self.field() if grad is None else grad

@@ -321,3 +321,40 @@ def test_narrow_pencil_tiles_are_bit_identical(spm, cuda, N, prec):
     assert np.array_equal(p8, p4) and np.array_equal(u8, u4)
     assert np.array_equal(h8, h4) and np.array_equal(w8, w4)
     assert rel(s4, s8) < (1e-12 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("N,prec,cps", [(64, "fp64", 2), (256, "fp64", 5), (256, "fp64", 6), (256, "fp32", 4)])
+def test_dependent_launches_are_bit_identical(spm, cuda, N, prec, cps):
+    """Plane and pencil kernels launched as programmatic dependents (knob pdl
+    1, the autotuner's choice at 256^3: a launch is set up while the previous
+    kernel of the stream completes, and the kernel waits on the device for it
+    before its first memory access) give the same bits as plain stream order
+    (pdl 0): a gradient chain with the 16-row and pipelined schedules, one that
+    stops inside a chain, a Hessian-vector block (several waves of clusters)
+    and the preconditioner. The grids are the same either way, so the step
+    records are equal too."""
+    phi = npo.uniform_field(N, 23)
+    V = np.stack([npo.uniform_field(N, 60 + i, amp=1.0) for i in range(3)])
+    dt = np.float64 if prec == "fp64" else np.float32
+    out = []
+    for pdl in (0, 1):
+        e = spm.SpmContext(N, Tau=-0.02, precision=prec)
+        e.tune("plane_cps", cps)
+        e.tune("plane_xg", 3)
+        e.tune("pdl", pdl)
+        assert e.tuning()["pdl"] == pdl
+        with pytest.raises(spm.SpmError):
+            e.tune("pdl", 2)
+        p = t(cuda, phi.astype(dt))
+        u = e.my_fft(p)
+        st = e.get_min_u_F(p, u, 19)
+        st2 = e.get_min_u_F(p, u, 3000, tol_grad=float(st[-1, 2]) * 0.5)
+        H = e.hv_cam(p, t(cuda, V.astype(dt)))
+        W = t(cuda, V.astype(dt))
+        e.precond_camnew(W)
+        out.append((st, st2, p.cpu().numpy(), u.cpu().numpy(), H.cpu().numpy(), W.cpu().numpy()))
+        e.close()
+    a, b = out
+    assert len(a[1]) == len(b[1]) < 3000
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
