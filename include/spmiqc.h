@@ -108,7 +108,7 @@ const char *spm_status_str(int status);
  * of more than 8 fields) stage their fields through shared memory with bulk
  * copies (1) or load them directly (0).
  * knob "pdl" (0 or 1): 1 = the plane and pencil kernels are launched as
- * programmatic dependents (not while the stream is being captured into a
+ * programmatic dependents (in a stream capture, programmatic edges of the
  * graph): a launch may be set up while the previous kernel of the stream
  * completes, and its kernel waits on the device for that kernel before its
  * first memory access; 0 (default) = plain stream order. The same bits

@@ -31,13 +31,9 @@ template <class Tag, class K> static cudaError_t prepare(K kern, size_t smem, in
   return e;
 }
 
-// Programmatic dependent launches (knob "pdl") on a stream that is not being
-// captured into a graph (captures keep plain stream order).
-static inline bool pdl_on(const spm_ctx *c) {
-  if (!c->pdl) return false;
-  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  return cudaStreamIsCapturing(c->stream, &st) == cudaSuccess && st == cudaStreamCaptureStatusNone;
-}
+// Programmatic dependent launches (knob "pdl"); a stream capture turns them
+// into programmatic edges of the graph.
+static inline bool pdl_on(const spm_ctx *c) { return c->pdl != 0; }
 
 // Persistent cluster launch: as many clusters as can be resident at once
 // (queried once per kernel and device), at most one per x-plane. With

@@ -54,14 +54,16 @@ def test_mixed_flow_matches_fp64_minimum(cuda):
     assert rel(b.cpu().numpy(), a.cpu().numpy()) < 1e-4  # both within ||grad F|| / |Tau| of the minimum
 
 
-@pytest.mark.parametrize("group", [1, 0])
-def test_batched_flows_match_single_flows(cuda, group):
+@pytest.mark.parametrize("group,pdl", [(1, 0), (0, 0), (1, 1), (0, 1)])
+def test_batched_flows_match_single_flows(cuda, group, pdl):
     """spm_batch_grad_flow over instances of different N and parameters gives,
     per instance, exactly the steps and state of a single flow (deterministic
     reductions: identical bits alone and in the batch), both when instances of
     one size share every launch (batch_group 1: three 32^3 instances with
     different L and Tau in one launch per pass, two 64^3 ones in another) and
-    when each instance has its own launches (batch_group 0)."""
+    when each instance has its own launches (batch_group 0); with pdl 1 the
+    captured graph's plane and pencil kernels are joined by programmatic edges
+    and the single flows run as dependent launches."""
     import ctypes
     import spmiqc
     lib = spmiqc.lib()
@@ -75,6 +77,7 @@ def test_batched_flows_match_single_flows(cuda, group):
     for N, L, tau, seed in specs:
         c = spmiqc.SpmContext(N, L=L, Tau=tau)
         c.tune("batch_group", group)
+        c.tune("pdl", pdl)
         p0 = npo.uniform_field(N, seed)
         p = cuda.from_numpy(p0).cuda()
         ctxs.append(c), phis.append(p), uhs.append(c.my_fft(p))
